@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark of the relational operator core on B200.
+
+Default workload (one "step"): hash group-by over 2^28 rows — int32 keys
+(scattered, uniform over --groups distinct values), an int64 column uniform
+in [0, 2^31) and a float64 column uniform in [0, 1), SUM / COUNT / MIN / MAX
+on both value columns (the group-by sweep configuration, one point of it).
+Inputs are generated on the device once and stay resident in HBM; they are
+5.4 GB, far larger than the 126 MB L2, so no L2 flush is needed between
+steps.  The sort-based join of 2^24 unique build keys with 2^28 probe keys
+(10% absent) is measured too and reported under "join".
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gx|reference]
+
+Prints one JSON line (rank 0).  `--impl reference` times the CPU restatement
+of the reference path (the oracle; the reference ships no CPU operators) on
+the host cores over a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "group-by & join Mrows/s at 2^28 rows, % HBM peak; batched+learned vs plain"
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Workload construction (device-side generators)
+# ---------------------------------------------------------------------------
+def make_groupby_inputs(gx, torch, rows: int, groups: int, seed: int):
+    k = torch.empty(rows, dtype=torch.int32, device="cuda")
+    gx.generate_keys(k, gx.gen_spec(seed=seed, stream_id=0, groups=groups, scatter=1))
+    iv = torch.empty(rows, dtype=torch.int64, device="cuda")
+    gx.generate_values(iv, gx.gen_spec(seed=seed, stream_id=1, lo=0, hi=1 << 31))
+    fv = torch.empty(rows, dtype=torch.float64, device="cuda")
+    gx.generate_values(fv, gx.gen_spec(seed=seed, stream_id=2))
+    return k, iv, fv
+
+
+REQS = None
+
+
+def groupby_reqs(gx):
+    return [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
+
+
+def time_steps(torch, fn, steps: int, warmup: int, dist=None) -> float:
+    """Device time (ms) of `steps` calls, CUDA events on the current stream."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(steps):
+        fn()
+    b.record(s)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def kernel_ms(gx, name: str) -> tuple[float, int]:
+    import ctypes
+    tot, cnt = ctypes.c_double(), ctypes.c_int64()
+    gx.check(gx.lib.gx_profile_read(name.encode(), ctypes.byref(tot), ctypes.byref(cnt)))
+    return tot.value, cnt.value
+
+
+def run_gx(args) -> None:
+    import torch
+    import eiger_b200 as gx
+    import ctypes
+
+    gx.lib.gx_profile_enable.argtypes = [ctypes.c_int32]
+    gx.lib.gx_profile_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+    gx.lib.gx_profile_reset.argtypes = []
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = dist_mod
+    else:
+        torch.cuda.set_device(0)
+    peaks = measured_peaks()
+    rows, G = args.rows, args.groups
+
+    # ----------------------------------------------------------- group-by
+    k, iv, fv = make_groupby_inputs(gx, torch, rows, G, seed=42 + rank)
+    reqs = groupby_reqs(gx)
+    hint_algo = {"hash": gx.HASH, "sort": gx.SORT, "partition": gx.PARTITION}[args.algo]
+
+    def step():
+        h = gx.make_hint(hint_algo, G)
+        return gx.groupby([k], [iv, fv], reqs, h)
+
+    res = step()
+    ngroups = res.num_rows
+    del res
+    launches0 = gx.kernel_launches()
+    gx.lib.gx_profile_reset()
+    gx.lib.gx_profile_enable(1)
+    with ClockSampler(local) as clk:
+        ms = time_steps(torch, step, args.steps, args.warmup, dist)
+    gx.lib.gx_profile_enable(0)
+    launches = gx.kernel_launches() - launches0
+    main_kernel = {"hash": "hash_groupby", "sort": "segmented_reduce", "partition": "partition_aggregate"}[args.algo]
+    kms, kcnt = kernel_ms(gx, main_kernel)
+    gx.lib.gx_profile_reset()
+    ms_step = ms / args.steps
+    value = world * rows / (ms_step * 1e-3) / 1e6
+    in_bytes = rows * (4 + 8 + 8)
+    out_bytes = ngroups * (4 + 8 * 7)
+    # The kernel's per-launch algorithmic bytes: key + value columns once.
+    k_launch_ms = kms / max(kcnt, 1)
+    achieved = in_bytes / (k_launch_ms * 1e-3) / 1e9 if kcnt else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": args.traffic,
+                "kernel": main_kernel, "kernel_ms": k_launch_ms, "peak_source": peaks["source"],
+                "operator_frac": (in_bytes + out_bytes) / (ms_step * 1e-3) / 1e9 / peaks["hbm_gbs"]}
+
+    # ------------------------------------------------------------- e2e
+    hk = torch.empty(rows, dtype=torch.int32, pin_memory=True)
+    hiv = torch.empty(rows, dtype=torch.int64, pin_memory=True)
+    hfv = torch.empty(rows, dtype=torch.float64, pin_memory=True)
+    hk.copy_(k)
+    hiv.copy_(iv)
+    hfv.copy_(fv)
+    del k, iv, fv
+    torch.cuda.empty_cache()
+
+    def e2e_step():
+        dk = hk.to("cuda", non_blocking=True)
+        div = hiv.to("cuda", non_blocking=True)
+        dfv = hfv.to("cuda", non_blocking=True)
+        t = gx.groupby([dk], [div, dfv], reqs, gx.make_hint(hint_algo, G))
+        cols = t.numpy_columns()  # device -> host read of the result
+        return cols
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_ms = time_steps(torch, e2e_step, e2e_steps, 1, dist) / e2e_steps
+    e2e = {"value": world * rows / (e2e_ms * 1e-3) / 1e6, "unit": "Mrows/s", "h2d_bytes_per_step": in_bytes,
+           "d2h_bytes_per_step": out_bytes, "ms_per_step": e2e_ms}
+    del hk, hiv, hfv
+    torch.cuda.empty_cache()
+
+    # ------------------------------------------------------------- join
+    join = None
+    if not args.no_join:
+        nb, npr = 1 << 24, args.join_rows
+        bk = torch.empty(nb, dtype=torch.int32, device="cuda")
+        gx.generate_permutation(bk, 42 + rank)
+        brow = torch.arange(nb, dtype=torch.int64, device="cuda")
+        pk = torch.empty(npr, dtype=torch.int32, device="cuda")
+        gx.generate_keys(pk, gx.gen_spec(seed=39 + rank, groups=nb, miss_frac=0.1))
+        prow = torch.arange(npr, dtype=torch.int64, device="cuda")
+        jh = gx.make_join_hint(gx.JOIN_SORT, gx.MAT_GFUR, unique_left=1)
+
+        def jstep():
+            return gx.inner_eq_join([bk, brow], [pk, prow], jh)
+
+        r = jstep()
+        matches = r.num_rows
+        del r
+        gx.lib.gx_profile_reset()
+        gx.lib.gx_profile_enable(1)
+        jms = time_steps(torch, jstep, max(1, args.steps // 2), 2, dist) / max(1, args.steps // 2)
+        gx.lib.gx_profile_enable(0)
+        wms, wc = kernel_ms(gx, "join_probe_write")
+        cms, cc = kernel_ms(gx, "join_probe_count")
+        gx.lib.gx_profile_reset()
+        probe_bytes = npr * (4 + 8) + matches * (4 + 8 + 8)
+        jalg = (nb + npr) * (4 + 8) + matches * (4 + 8 + 8)
+        join = {"workload": "sort-based inner equi-join, 2^24 unique int32 build keys (int64 payload) x "
+                            f"{npr} int32 probe keys (10% absent, int64 payload)",
+                "value": world * (nb + npr) / (jms * 1e-3) / 1e6, "unit": "Mrows/s", "ms_per_step": jms,
+                "matches": matches,
+                "probe_write_ms": wms / max(wc, 1), "probe_count_ms": cms / max(cc, 1),
+                "probe_frac": probe_bytes / ((wms / max(wc, 1) + cms / max(cc, 1)) * 1e-3) / 1e9 / peaks["hbm_gbs"]
+                if wc else None,
+                "operator_frac": jalg / (jms * 1e-3) / 1e9 / peaks["hbm_gbs"]}
+        del bk, brow, pk, prow
+
+    # ------------------------------------------------------ cpu baseline
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_groupby_baseline(args.cpu_rows, G)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+            "config": {"workload": f"hash group-by, {rows} rows, int32 keys uniform over {G} scattered values, "
+                                   "int64 [0,2^31) + float64 [0,1) values, SUM/COUNT/MIN/MAX on both",
+                       "rows": rows, "groups": G, "groups_found": ngroups, "algo": args.algo,
+                       "l2": "inputs (5.4 GB) larger than L2; no flush"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk.summary(), "join": join,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_groupby_baseline(rows: int, groups: int) -> dict:
+    """The oracle (CPU restatement, all host threads) on a bounded sample."""
+    import oracle as O
+    k = O.gen_keys(rows, np.int32, groups=groups, scatter=1, seed=42)
+    iv = O.gen_values(rows, np.int64, seed=42, stream_id=1, lo=0, hi=1 << 31)
+    fv = O.gen_values(rows, np.float64, seed=42, stream_id=2)
+    reqs = [(0, O.SUM), (0, O.MIN), (0, O.MAX), (1, O.SUM), (1, O.MIN), (1, O.MAX), (0, O.COUNT_ALL)]
+    t0 = time.perf_counter()
+    O.groupby(k, [iv, fv], reqs)
+    dt = time.perf_counter() - t0
+    return {"value": rows / dt / 1e6, "unit": "Mrows/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{rows} rows of the same workload (oracle hash group-by, sorted output)"}
+
+
+def run_reference(args) -> None:
+    """CPU restatement of the reference path, host cores, bounded samples."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle as O
+    rows = args.cpu_rows
+    G = args.groups
+    k = O.gen_keys(rows, np.int32, groups=G, scatter=1, seed=42)
+    iv = O.gen_values(rows, np.int64, seed=42, stream_id=1, lo=0, hi=1 << 31)
+    fv = O.gen_values(rows, np.float64, seed=42, stream_id=2)
+    reqs = [(0, O.SUM), (0, O.MIN), (0, O.MAX), (1, O.SUM), (1, O.MIN), (1, O.MAX), (0, O.COUNT_ALL)]
+    for _ in range(args.warmup):
+        O.groupby(k, [iv, fv], reqs)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.groupby(k, [iv, fv], reqs)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = rows / dt / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+            "config": {"workload": f"hash group-by, {args.rows} rows, int32 keys uniform over {G} scattered "
+                                   "values, int64 + float64 values, SUM/COUNT/MIN/MAX on both",
+                       "rows": args.rows, "groups": G, "sample_rows": rows},
+            "cpu_baseline": {"value": value, "unit": "Mrows/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": f"{rows} rows per step (the reference has no CPU operators; this is "
+                                       "the CPU restatement of its group-by)"},
+            "e2e": {"value": value, "unit": "Mrows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["gx", "reference"], default="gx")
+    ap.add_argument("--rows", type=int, default=1 << 28)
+    ap.add_argument("--groups", type=int, default=1 << 16)
+    ap.add_argument("--algo", choices=["hash", "sort", "partition"], default="hash")
+    ap.add_argument("--join-rows", type=int, default=1 << 28)
+    ap.add_argument("--no-join", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-rows", type=int, default=1 << 24)
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="dram bytes per launch of the dominant kernel from an ncu capture")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gx(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,340 @@
+// gx_core.cuh — shared host/device infrastructure of the operator core:
+// status/exception plumbing for the C ABI, the stream-ordered pool
+// allocator, owned columns/tables, type helpers, hashing and small device
+// primitives (warp/block scans, order-preserving key images).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/gx.h"
+
+namespace gx {
+
+// ---------------------------------------------------------------------------
+// Errors. C++ code throws gx::error; the C ABI layer catches and converts to
+// a gx_status plus a thread-local message (reference: std::runtime_error /
+// std::bad_alloc, src/cuda/operators/groupby/groupby.cu:287-299).
+// ---------------------------------------------------------------------------
+struct error : std::runtime_error {
+    gx_status status;
+    error(gx_status s, const std::string& msg) : std::runtime_error(msg), status(s) {}
+};
+
+[[noreturn]] inline void fail(gx_status s, const std::string& msg) { throw error(s, msg); }
+inline void require(bool ok, const std::string& msg) {
+    if (!ok) fail(GX_EINVAL, msg);
+}
+
+inline void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
+    if (e != cudaSuccess) {
+        fail(e == cudaErrorMemoryAllocation ? GX_ENOMEM : GX_ECUDA,
+             std::string(what) + " failed: " + cudaGetErrorString(e) + " at " + file + ":" +
+                 std::to_string(line));
+    }
+}
+#define GX_CUDA(call) ::gx::cuda_check((call), #call, __FILE__, __LINE__)
+
+// Every kernel launch goes through this counter so callers can verify which
+// work ran on the device (gx_kernel_launch_count).
+extern std::atomic<int64_t> g_launches;
+#define GX_LAUNCHED()                                          \
+    do {                                                       \
+        ::gx::g_launches.fetch_add(1, std::memory_order_relaxed); \
+        GX_CUDA(cudaGetLastError());                           \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Optional per-kernel timing with CUDA events on the launching stream
+// (gx_profile_enable / gx_profile_read).  A scope records an event pair
+// around the launches it encloses when profiling is on.
+// ---------------------------------------------------------------------------
+extern std::atomic<int> g_profiling;
+struct prof_scope {
+    const char* name;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr, b = nullptr;
+    prof_scope(const char* n, cudaStream_t st);
+    ~prof_scope();
+};
+#define GX_PROF_CAT2(a, b) a##b
+#define GX_PROF_CAT(a, b) GX_PROF_CAT2(a, b)
+#define GX_PROF(name, stream) ::gx::prof_scope GX_PROF_CAT(_gx_prof_, __LINE__)(name, stream)
+void prof_read(const char* name, double* total_ms, int64_t* count, bool reset);
+
+// ---------------------------------------------------------------------------
+// Device properties (cached per device).
+// ---------------------------------------------------------------------------
+struct device_info {
+    int device = 0;
+    int sm_count = 148;
+    int max_smem_optin = 227 * 1024;
+    int l2_bytes = 126 * 1024 * 1024;
+};
+const device_info& dev();
+
+// ---------------------------------------------------------------------------
+// Stream-ordered pool allocator (cudaMallocAsync on the device's default
+// pool with the release threshold raised so freed blocks stay cached).
+// Replaces the reference's first-fit slab (src/cuda/memory/mem_manager.cu:33-231).
+// ---------------------------------------------------------------------------
+void* pool_alloc(size_t bytes, cudaStream_t s);
+void pool_free(void* p, cudaStream_t s);
+void pool_stats(int64_t* cur, int64_t* peak);
+void pool_reset_peak();
+
+// RAII device buffer bound to a stream.
+class dbuf {
+public:
+    dbuf() = default;
+    dbuf(size_t bytes, cudaStream_t s) : s_(s), bytes_(bytes) {
+        p_ = bytes ? pool_alloc(bytes, s) : nullptr;
+    }
+    ~dbuf() { reset(); }
+    dbuf(const dbuf&) = delete;
+    dbuf& operator=(const dbuf&) = delete;
+    dbuf(dbuf&& o) noexcept : p_(o.p_), s_(o.s_), bytes_(o.bytes_) { o.p_ = nullptr; o.bytes_ = 0; }
+    dbuf& operator=(dbuf&& o) noexcept {
+        if (this != &o) { reset(); p_ = o.p_; s_ = o.s_; bytes_ = o.bytes_; o.p_ = nullptr; o.bytes_ = 0; }
+        return *this;
+    }
+    void reset() {
+        if (p_) pool_free(p_, s_);
+        p_ = nullptr;
+        bytes_ = 0;
+    }
+    void* release() { void* p = p_; p_ = nullptr; bytes_ = 0; return p; }
+    template <typename T = void>
+    T* get() const { return static_cast<T*>(p_); }
+    size_t bytes() const { return bytes_; }
+
+private:
+    void* p_ = nullptr;
+    cudaStream_t s_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Types.
+// ---------------------------------------------------------------------------
+inline int size_of(int t) {
+    switch (t) {
+        case GX_INT8: case GX_UINT8: case GX_BOOL8: return 1;
+        case GX_INT16: case GX_UINT16: return 2;
+        case GX_INT32: case GX_UINT32: case GX_FLOAT32: return 4;
+        case GX_INT64: case GX_UINT64: case GX_FLOAT64: return 8;
+        default: return 0;
+    }
+}
+inline bool is_signed_int(int t) { return t == GX_INT8 || t == GX_INT16 || t == GX_INT32 || t == GX_INT64; }
+inline bool is_unsigned_int(int t) {
+    return t == GX_UINT8 || t == GX_UINT16 || t == GX_UINT32 || t == GX_UINT64 || t == GX_BOOL8;
+}
+inline bool is_float(int t) { return t == GX_FLOAT32 || t == GX_FLOAT64; }
+inline bool is_numeric(int t) { return size_of(t) > 0; }
+std::string type_name(int t);
+
+// Value "kind" used inside kernels: how raw bits widen to a 64-bit lane.
+enum vkind : int { VK_I = 0, VK_U = 1, VK_F = 2 };
+inline int vkind_of(int t) { return is_float(t) ? VK_F : (is_signed_int(t) ? VK_I : VK_U); }
+
+// A resolved column: base pointer already advanced by the view offset.
+struct col {
+    const void* data = nullptr;
+    int64_t n = 0;
+    int type = GX_EMPTY;
+    template <typename T>
+    const T* as() const { return static_cast<const T*>(data); }
+};
+inline col resolve(const gx_column_view& v) {
+    col c;
+    c.type = v.type;
+    c.n = v.size;
+    int w = size_of(v.type);
+    c.data = v.data ? static_cast<const char*>(v.data) + v.offset * (int64_t)(w ? w : 1) : nullptr;
+    require(v.size >= 0, "negative column size");
+    require(v.offset >= 0, "negative column offset");
+    return c;
+}
+
+// ---------------------------------------------------------------------------
+// Owned columns / tables returned through the C ABI.
+// ---------------------------------------------------------------------------
+struct owned_col {
+    dbuf buf;
+    int64_t size = 0;
+    int type = GX_EMPTY;
+    bool present = true;
+};
+
+}  // namespace gx
+
+struct gx_table {
+    std::vector<gx::owned_col> cols;
+};
+
+namespace gx {
+
+inline owned_col make_col(int type, int64_t rows, cudaStream_t s, int64_t capacity_rows = -1) {
+    owned_col c;
+    c.type = type;
+    c.size = rows;
+    int64_t cap = capacity_rows < 0 ? rows : capacity_rows;
+    size_t bytes = (size_t)cap * size_of(type);
+    if (bytes) c.buf = dbuf(bytes, s);
+    return c;
+}
+inline gx_column to_gx_column(owned_col&& c) {
+    gx_column out;
+    out.size = c.size;
+    out.type = c.type;
+    out.capacity_bytes = (int64_t)c.buf.bytes();
+    out.data = c.buf.release();
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// Hashing: MurmurHash3 fmix32/fmix64 finalizers (public algorithm; the
+// reference uses the same finalizers for partition ids,
+// src/cuda/operators/groupby/groupby_partition.cu:64-89).
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t x) {
+    x ^= x >> 16; x *= 0x85ebca6bU; x ^= x >> 13; x *= 0xc2b2ae35U; x ^= x >> 16;
+    return x;
+}
+__host__ __device__ __forceinline__ uint64_t fmix64(uint64_t x) {
+    x ^= x >> 33; x *= 0xff51afd7ed558ccdULL; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ULL; x ^= x >> 33;
+    return x;
+}
+
+// Canonical equality image of a key's raw bits: float -0.0 and +0.0 compare
+// equal (the reference compares keys with operator==), so they map to the
+// same bits.  `kind`: VK_I/VK_U keep the bits, VK_F normalises zero.
+__host__ __device__ __forceinline__ uint32_t canon32(uint32_t b, int kind) {
+    return (kind == VK_F && (b << 1) == 0u) ? 0u : b;
+}
+__host__ __device__ __forceinline__ uint64_t canon64(uint64_t b, int kind) {
+    return (kind == VK_F && (b << 1) == 0ull) ? 0ull : b;
+}
+
+// Order-preserving unsigned image of a key (radix sort digit source):
+// signed ints flip the sign bit, floats flip all bits when negative and the
+// sign bit otherwise (-0.0 first normalised to +0.0), unsigned unchanged.
+__host__ __device__ __forceinline__ uint32_t ordered32(uint32_t b, int kind) {
+    if (kind == VK_I) return b ^ 0x80000000u;
+    if (kind == VK_F) {
+        if (b == 0x80000000u) b = 0u;
+        return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    }
+    return b;
+}
+__host__ __device__ __forceinline__ uint64_t ordered64(uint64_t b, int kind) {
+    if (kind == VK_I) return b ^ 0x8000000000000000ull;
+    if (kind == VK_F) {
+        if (b == 0x8000000000000000ull) b = 0ull;
+        return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+    }
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// Small helpers.
+// ---------------------------------------------------------------------------
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+inline int ilog2_ceil(uint64_t x) {
+    int b = 0;
+    while ((uint64_t(1) << b) < x) ++b;
+    return b;
+}
+inline uint64_t next_pow2(uint64_t x) { return x <= 1 ? 1 : (uint64_t(1) << ilog2_ceil(x)); }
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Host <- device copy of a small value with a stream sync.
+template <typename T>
+T read_scalar(const T* dptr, cudaStream_t s) {
+    T v;
+    GX_CUDA(cudaMemcpyAsync(&v, dptr, sizeof(T), cudaMemcpyDeviceToHost, s));
+    GX_CUDA(cudaStreamSynchronize(s));
+    return v;
+}
+
+// Grid size for a grid-stride kernel: a multiple of the SM count.
+inline int grid_for(int64_t work_items, int per_block, int blocks_per_sm = 4) {
+    int64_t need = ceil_div(work_items > 0 ? work_items : 1, per_block);
+    int64_t cap = (int64_t)dev().sm_count * blocks_per_sm;
+    return (int)(need < cap ? need : cap);
+}
+
+// Fill a device buffer of 8-byte words with a pattern (kernel in gx_util.cu).
+void fill_u64(void* dst, uint64_t pattern, int64_t words, cudaStream_t s);
+void fill_u32(void* dst, uint32_t pattern, int64_t words, cudaStream_t s);
+// Exclusive scan of int64 counts into offsets (n+1 outputs, out[n] = total).
+void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
+// iota of int64.
+void sequence_i64(int64_t* out, int64_t n, int64_t start, int64_t step, cudaStream_t s);
+// out[i] = src[idx[i]] for `width`-byte elements.
+void gather_bytes(void* out, const void* src, const int64_t* idx, int64_t n, int width,
+                  cudaStream_t s);
+// Widen a 1/2-byte integer column to 4 bytes (sign- or zero-extended).
+owned_col widen_to_32(const col& c, cudaStream_t s);
+
+}  // namespace gx
+
+// ---------------------------------------------------------------------------
+// Device-side helpers.
+// ---------------------------------------------------------------------------
+#ifdef __CUDACC__
+namespace gx {
+namespace dev_ {
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// Inclusive warp scan.
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_sum(T v) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane_id() >= o) v += n;
+    }
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide exclusive scan for blockDim.x == NT (multiple of 32).
+// `smem` needs NT/32 + 1 slots.  Returns exclusive prefix; *total gets the sum.
+template <int NT, typename T>
+__device__ __forceinline__ T block_exclusive_sum(T v, T* smem, T* total) {
+    const int warp = threadIdx.x >> 5;
+    T inc = warp_inclusive_sum(v);
+    if (lane_id() == 31) smem[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane_id() < NT / 32 ? smem[lane_id()] : T(0);
+        T wi = warp_inclusive_sum(w);
+        if (lane_id() < NT / 32) smem[lane_id()] = wi - w;
+        if (lane_id() == NT / 32 - 1) smem[NT / 32] = wi;
+    }
+    __syncthreads();
+    T res = smem[warp] + inc - v;
+    *total = smem[NT / 32];
+    __syncthreads();
+    return res;
+}
+
+}  // namespace dev_
+}  // namespace gx
+#endif

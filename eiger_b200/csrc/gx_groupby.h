@@ -1,0 +1,43 @@
+// gx_groupby.h — internal interfaces between the operator translation units.
+#pragma once
+
+#include "gx_agg.cuh"
+
+namespace gx {
+
+// ----- hash group-by (gx_groupby_hash.cu) -----
+void init_records(uint64_t* recs, int64_t nrec, const agg_desc& d, uint64_t empty, cudaStream_t s);
+int hash_smem_slots(const agg_desc& d, int key_width, int64_t groups_bound);
+void hash_groupby(const col& key, const agg_plan& p, gx_groupby_hint* hint, cudaStream_t s,
+                  gx_table* out);
+
+// ----- sort / partition group-by (gx_groupby_sort.cu, gx_groupby_partition.cu) -----
+void sort_groupby(const col& key, const agg_plan& p, gx_groupby_hint* hint, bool gfur,
+                  cudaStream_t s, gx_table* out);
+void partition_groupby(const col& key, const agg_plan& p, gx_groupby_hint* hint, bool gfur,
+                       cudaStream_t s, gx_table* out);
+
+// ----- radix sort / partition (gx_radix.cu) -----
+// Stable LSD radix sort of (key, value) on bits [begin_bit, end_bit) of the
+// order-preserving key image.  vals_in may be null (keys only) or, with
+// vals_iota, the values are the row ids 0..n-1 (int64).  Outputs are
+// caller-allocated.  Key types: any numeric; value widths 4 or 8 (or 0).
+struct radix_temp {
+    dbuf own;
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+size_t radix_temp_bytes(int64_t n, int key_width, int val_width);
+void radix_sort(const col& keys, const void* vals_in, int val_width, bool vals_iota,
+                int begin_bit, int end_bit, bool descending, void* keys_out, void* vals_out,
+                void* temp, size_t temp_bytes, cudaStream_t s);
+// Key image width in bits for a type (the default end_bit).
+inline int key_bits(int type) { return 8 * size_of(type); }
+
+// Min/max of the order-preserving image (for trimming radix passes).
+void key_image_range(const col& keys, uint64_t* lo, uint64_t* hi, cudaStream_t s);
+
+// ----- statistics (gx_hll.cu) -----
+int64_t ndv_estimate(const col& key, cudaStream_t s);
+
+}  // namespace gx

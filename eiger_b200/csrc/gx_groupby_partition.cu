@@ -1,0 +1,521 @@
+// gx_groupby_partition.cu — partition-based group-by (PARTITION, PARTITION_GFUR).
+//
+// Replaces gamax::groupby::partition::groupby / groupby_gfur
+// (src/cuda/operators/groupby/groupby_partition.cu:557-707).  Same shape as
+// the reference — hash-partition the rows so each partition's groups fit a
+// shared-memory table, then aggregate one partition per CTA — with three
+// changes:
+//   * partition id = fmix(key) on R radix bits (R chosen from the group
+//     estimate, or hint.radix_bits) instead of a fixed 16; rows are moved by
+//     one multi-column scatter per 8-bit digit (GFTR moves key + every value
+//     column, GFUR key + row id) instead of one CUB sort per column;
+//   * partitions larger than a threshold are split into work units so a
+//     Zipf-hot partition is spread over many CTAs (the reference assigns one
+//     CTA per partition, groupby_partition.cu:433);
+//   * a partition whose distinct keys overflow its shared table spills to a
+//     global table instead of throwing (groupby_partition.cu:543-549).
+#include <algorithm>
+
+#include "gx_groupby.h"
+
+namespace gx {
+namespace {
+
+constexpr int PS_NT = 512;
+constexpr int PS_WARPS = PS_NT / 32;
+constexpr int PS_IPT = 8;
+constexpr int PS_TILE = PS_NT * PS_IPT;
+constexpr int PS_BINS = 256;
+
+template <int KW>
+__device__ __forceinline__ uint32_t part_hash(uint64_t kb) {
+    if (KW == 4) return fmix32((uint32_t)kb);
+    uint64_t h = fmix64(kb);
+    return (uint32_t)(h ^ (h >> 32));
+}
+template <int KW>
+__device__ __forceinline__ uint64_t ld_key(const void* p, int64_t i, int kind) {
+    if (KW == 4) return canon32(__ldg(static_cast<const unsigned*>(p) + i), kind);
+    return canon64(__ldg(static_cast<const unsigned long long*>(p) + i), kind);
+}
+
+template <int KW>
+__global__ void __launch_bounds__(PS_NT) k_part_hist(const void* __restrict__ keys, int64_t n, int kind,
+                                                      int shift, int dbits, int64_t ntiles,
+                                                      int64_t* __restrict__ counts) {
+    __shared__ unsigned hist[PS_BINS];
+    const int bins = 1 << dbits;
+    for (int b = threadIdx.x; b < bins; b += PS_NT) hist[b] = 0;
+    __syncthreads();
+    int64_t base = blockIdx.x * (int64_t)PS_TILE;
+#pragma unroll
+    for (int k = 0; k < PS_IPT; ++k) {
+        int64_t i = base + k * PS_NT + threadIdx.x;
+        if (i < n) atomicAdd(&hist[(part_hash<KW>(ld_key<KW>(keys, i, kind)) >> shift) & (bins - 1)], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < bins; b += PS_NT) counts[(int64_t)b * ntiles + blockIdx.x] = hist[b];
+}
+
+struct move_cols {
+    int n;
+    const void* in[MAX_VCOLS + 2];
+    void* out[MAX_VCOLS + 2];
+    int width[MAX_VCOLS + 2];
+    int iota[MAX_VCOLS + 2];  // 1: the column is the row id (input ignored)
+};
+
+// Stable multi-column scatter by one hash digit: ranks are computed once with
+// a warp multisplit, then each column is staged through shared memory in
+// digit order and written out in contiguous runs.
+template <int KW>
+__global__ void __launch_bounds__(PS_NT) k_part_scatter(const void* __restrict__ keys, int64_t n, int kind,
+                                                         int shift, int dbits, int64_t ntiles,
+                                                         const int64_t* __restrict__ offsets, move_cols mc) {
+    __shared__ unsigned whist[PS_WARPS * PS_BINS];
+    __shared__ int64_t gbase[PS_BINS];
+    __shared__ unsigned dbase[PS_BINS];
+    extern __shared__ __align__(16) unsigned long long part_dyn[];
+    unsigned long long* stage = part_dyn;                                        // [PS_TILE]
+    unsigned short* sdig = reinterpret_cast<unsigned short*>(part_dyn + PS_TILE);  // [PS_TILE]
+
+    const int bins = 1 << dbits;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < PS_WARPS * PS_BINS; i += PS_NT) whist[i] = 0;
+    __syncthreads();
+    const int64_t tile_base = blockIdx.x * (int64_t)PS_TILE;
+    const int tile_n = (int)min((int64_t)PS_TILE, n - tile_base);
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned dig[PS_IPT], rank[PS_IPT];
+#pragma unroll
+    for (int k = 0; k < PS_IPT; ++k) {
+        int local = warp * 32 * PS_IPT + k * 32 + lane;
+        bool valid = local < tile_n;
+        unsigned d = valid ? (part_hash<KW>(ld_key<KW>(keys, tile_base + local, kind)) >> shift) & (bins - 1) : 0xFFFFu;
+        dig[k] = d;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        unsigned r = __popc(peers & lt);
+        unsigned prior = valid ? whist[warp * PS_BINS + d] : 0;
+        rank[k] = prior + r;
+        __syncwarp();
+        if (valid && r == 0) whist[warp * PS_BINS + d] = prior + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    if (threadIdx.x < PS_BINS) {
+        unsigned run = 0;
+        if ((int)threadIdx.x < bins)
+            for (int w = 0; w < PS_WARPS; ++w) {
+                unsigned c = whist[w * PS_BINS + threadIdx.x];
+                whist[w * PS_BINS + threadIdx.x] = run;
+                run += c;
+            }
+        dbase[threadIdx.x] = run;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned v[PS_BINS / 32], s = 0;
+#pragma unroll
+        for (int j = 0; j < PS_BINS / 32; ++j) { v[j] = dbase[lane * (PS_BINS / 32) + j]; s += v[j]; }
+        unsigned run = dev_::warp_inclusive_sum(s) - s;
+#pragma unroll
+        for (int j = 0; j < PS_BINS / 32; ++j) { dbase[lane * (PS_BINS / 32) + j] = run; run += v[j]; }
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < bins)
+        gbase[threadIdx.x] = offsets[(int64_t)threadIdx.x * ntiles + blockIdx.x] - (int64_t)dbase[threadIdx.x];
+    unsigned pos[PS_IPT];
+#pragma unroll
+    for (int k = 0; k < PS_IPT; ++k) {
+        int local = warp * 32 * PS_IPT + k * 32 + lane;
+        if (local < tile_n) {
+            pos[k] = dbase[dig[k]] + whist[warp * PS_BINS + dig[k]] + rank[k];
+            sdig[pos[k]] = (unsigned short)dig[k];
+        }
+    }
+    for (int c = 0; c < mc.n; ++c) {
+        __syncthreads();
+        const int w = mc.width[c];
+#pragma unroll
+        for (int k = 0; k < PS_IPT; ++k) {
+            int local = warp * 32 * PS_IPT + k * 32 + lane;
+            if (local < tile_n) {
+                int64_t i = tile_base + local;
+                unsigned long long x;
+                if (mc.iota[c]) x = (unsigned long long)i;
+                else if (w == 8) x = __ldg(static_cast<const unsigned long long*>(mc.in[c]) + i);
+                else x = __ldg(static_cast<const unsigned*>(mc.in[c]) + i);
+                stage[pos[k]] = x;
+            }
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < tile_n; j += PS_NT) {
+            int64_t o = gbase[sdig[j]] + j;
+            if (w == 8) static_cast<unsigned long long*>(mc.out[c])[o] = stage[j];
+            else static_cast<unsigned*>(mc.out[c])[o] = (unsigned)stage[j];
+        }
+    }
+}
+
+// Work units: partition p split into ceil(size/T) units.
+__global__ void k_unit_counts(const int64_t* __restrict__ part_start, int P, int64_t T,
+                              int64_t* __restrict__ ucount) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < P) {
+        int64_t sz = part_start[p + 1] - part_start[p];
+        ucount[p] = sz == 0 ? 0 : (sz + T - 1) / T;
+    }
+}
+struct unit { int64_t begin, end; int split; int pad; };
+__global__ void k_unit_fill(const int64_t* __restrict__ part_start, const int64_t* __restrict__ uoff, int P,
+                            int64_t T, unit* __restrict__ units) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    int64_t b = part_start[p], e = part_start[p + 1];
+    int64_t u0 = uoff[p], nu = uoff[p + 1] - u0;
+    for (int64_t u = 0; u < nu; ++u) {
+        unit x;
+        x.begin = b + u * T;
+        x.end = min(e, x.begin + T);
+        x.split = nu > 1;
+        x.pad = 0;
+        units[u0 + u] = x;
+    }
+}
+
+constexpr uint64_t PG_EMPTY4 = ~0ull;
+constexpr uint64_t PG_EMPTY8 = 0x8000000000000000ull;
+constexpr int PA_NT = 512;
+
+struct pglobal {
+    uint64_t* recs;  // (cap + 1) records, the last one for the key equal to the empty marker
+    uint64_t mask;
+    int* sentinel_flag;
+    int* overflow;
+};
+
+template <int KW>
+__device__ __forceinline__ uint64_t* pg_find(const pglobal& t, const agg_desc& d, uint64_t kw, uint32_t h) {
+    const uint64_t EMPTY = KW == 4 ? PG_EMPTY4 : PG_EMPTY8;
+    if (KW == 8 && kw == EMPTY) {
+        atomicExch(t.sentinel_flag, 1);
+        return t.recs + (t.mask + 1) * d.rec_words;
+    }
+    uint64_t slot = (h * 0x9E3779B1u) & t.mask;
+    for (uint64_t p = 0; p <= t.mask; ++p) {
+        uint64_t* r = t.recs + slot * d.rec_words;
+        uint64_t cur = *(volatile uint64_t*)r;
+        if (cur == kw) return r;
+        if (cur == EMPTY) {
+            unsigned long long old = atomicCAS((unsigned long long*)r, (unsigned long long)EMPTY, (unsigned long long)kw);
+            if (old == EMPTY || old == kw) return r;
+        }
+        slot = (slot + 1) & t.mask;
+    }
+    atomicExch(t.overflow, 1);
+    return nullptr;
+}
+
+// One CTA per work unit (grid-stride over units).  Shared table layout:
+// keys[S] (u64) | counts[S] (u32) | acc[A][S] (u64).
+template <int KW>
+__global__ void __launch_bounds__(PA_NT) k_part_agg(const void* __restrict__ pkeys,
+                                                     const int64_t* __restrict__ prow,  // GFUR row ids (or null)
+                                                     move_cols pvals,                  // GFTR partitioned values
+                                                     int kind, agg_desc d, const unit* __restrict__ units,
+                                                     const int64_t* __restrict__ n_units, uint32_t S, int rbits,
+                                                     pglobal g, uint64_t* __restrict__ out_recs,
+                                                     unsigned long long* __restrict__ out_count) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_fill;
+    __shared__ unsigned long long s_base;
+    unsigned long long* skeys = reinterpret_cast<unsigned long long*>(smem);
+    unsigned* scnt = reinterpret_cast<unsigned*>(smem + (size_t)S * 8);
+    uint64_t* sacc = reinterpret_cast<uint64_t*>(smem + (size_t)S * 12);
+    const uint64_t EMPTY = KW == 4 ? PG_EMPTY4 : PG_EMPTY8;
+    const uint32_t mask = S - 1;
+    const int limit = (int)(S - S / 4);
+    const int64_t nu = *n_units;
+    for (int64_t u = blockIdx.x; u < nu; u += gridDim.x) {
+        const unit un = units[u];
+        for (uint32_t i = threadIdx.x; i < S; i += PA_NT) { skeys[i] = EMPTY; scnt[i] = 0; }
+        for (int a = 0; a < d.n_acc; ++a) {
+            int op = d.acc_op[a], kd = d.acc_kind[a];
+            uint64_t idv = op == OP_MIN ? (kd == VK_I ? 0x7FFFFFFFFFFFFFFFull : (kd == VK_U ? ~0ull : 0x7FF0000000000000ull))
+                         : op == OP_MAX ? (kd == VK_I ? 0x8000000000000000ull : (kd == VK_U ? 0ull : 0xFFF0000000000000ull))
+                         : 0ull;
+            for (uint32_t i = threadIdx.x; i < S; i += PA_NT) sacc[(size_t)a * S + i] = idv;
+        }
+        if (threadIdx.x == 0) s_fill = 0;
+        __syncthreads();
+        for (int64_t i = un.begin + threadIdx.x; i < un.end; i += PA_NT) {
+            uint64_t kw = ld_key<KW>(pkeys, i, kind);
+            uint32_t h = part_hash<KW>(kw);
+            uint64_t v[MAX_VCOLS];
+            if (prow) {
+                int64_t src = prow[i];
+#pragma unroll
+                for (int c = 0; c < MAX_VCOLS; ++c)
+                    if (c < d.n_cols) v[c] = dev_::load_lane(d.col_ptr[c], d.col_width[c], d.col_kind[c], src);
+            } else {
+#pragma unroll
+                for (int c = 0; c < MAX_VCOLS; ++c)
+                    if (c < d.n_cols) v[c] = dev_::load_lane(pvals.out[c], d.col_width[c], d.col_kind[c], i);
+            }
+            // Slot from the hash bits above the partition bits.
+            uint32_t slot = (h >> rbits) & mask;
+            int found = -1;
+            if (!(KW == 8 && kw == EMPTY)) {
+                for (uint32_t p = 0; p <= mask; ++p) {
+                    unsigned long long cur = ((volatile unsigned long long*)skeys)[slot];
+                    if (cur == kw) { found = (int)slot; break; }
+                    if (cur == EMPTY) {
+                        if (*(volatile int*)&s_fill >= limit) break;
+                        unsigned long long old = atomicCAS(&skeys[slot], (unsigned long long)EMPTY, (unsigned long long)kw);
+                        if (old == EMPTY) { atomicAdd(&s_fill, 1); found = (int)slot; break; }
+                        if (old == kw) { found = (int)slot; break; }
+                    }
+                    slot = (slot + 1) & mask;
+                }
+            }
+            if (found >= 0) {
+                if (d.has_count) atomicAdd(&scnt[found], 1u);
+                for (int a = 0; a < d.n_acc; ++a)
+                    dev_::acc_atomic(sacc + (size_t)a * S + found, d.acc_op[a], d.acc_kind[a], dev_::pick(v, d.acc_col[a]));
+            } else {
+                uint64_t* r = pg_find<KW>(g, d, kw, h);
+                if (r) {
+                    if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), 1ull);
+                    for (int a = 0; a < d.n_acc; ++a)
+                        dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], dev_::pick(v, d.acc_col[a]));
+                }
+            }
+        }
+        __syncthreads();
+        if (!un.split) {
+            // Whole partition in this CTA: its groups are final; append them densely.
+            if (threadIdx.x == 0) s_base = atomicAdd(out_count, (unsigned long long)s_fill);
+            __syncthreads();
+            // Compact occupied slots in slot order with a block scan.
+            __shared__ int64_t scan_sm[PA_NT / 32 + 1];
+            int64_t running = 0;
+            for (uint32_t i0 = 0; i0 < S; i0 += PA_NT) {
+                uint32_t i = i0 + threadIdx.x;
+                bool live = i < S && skeys[i] != EMPTY;
+                int64_t tot;
+                int64_t ex = dev_::block_exclusive_sum<PA_NT, int64_t>(live ? 1 : 0, scan_sm, &tot);
+                if (live) {
+                    uint64_t* r = out_recs + (s_base + running + ex) * d.rec_words;
+                    r[0] = skeys[i];
+                    if (d.has_count) r[d.count_word] = scnt[i];
+                    for (int a = 0; a < d.n_acc; ++a) r[d.acc_word0 + a] = sacc[(size_t)a * S + i];
+                }
+                running += tot;
+            }
+        } else {
+            for (uint32_t i = threadIdx.x; i < S; i += PA_NT) {
+                unsigned long long k = skeys[i];
+                if (k == EMPTY) continue;
+                uint64_t* r = pg_find<KW>(g, d, k, part_hash<KW>(k));
+                if (!r) continue;
+                if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), (unsigned long long)scnt[i]);
+                for (int a = 0; a < d.n_acc; ++a)
+                    dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], sacc[(size_t)a * S + i]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Append the occupied records of the global spill table after the dense ones.
+__global__ void k_append_global(const uint64_t* __restrict__ g, int64_t cap, int rec_words, uint64_t empty,
+                                const int* __restrict__ sentinel_flag, uint64_t* __restrict__ out,
+                                unsigned long long* __restrict__ out_count) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r <= cap; r += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t* src = g + r * rec_words;
+        bool live = r < cap ? src[0] != empty : *sentinel_flag != 0;
+        if (!live) continue;
+        unsigned long long pos = atomicAdd(out_count, 1ull);
+        for (int w = 0; w < rec_words; ++w) out[pos * rec_words + w] = src[w];
+    }
+}
+
+}  // namespace
+
+void partition_starts(const void* keys, int kw, int64_t n, int kind, int R, int64_t* ps, cudaStream_t s);
+
+namespace {
+
+template <int KW>
+void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_cols& mc, int64_t* counts,
+               int64_t* offs, cudaStream_t s) {
+    int64_t ntiles = ceil_div(n, PS_TILE);
+    k_part_hist<KW><<<(unsigned)ntiles, PS_NT, 0, s>>>(kin, n, kind, shift, dbits, ntiles, counts);
+    GX_LAUNCHED();
+    exclusive_scan_i64(counts, offs, ((int64_t)1 << dbits) * ntiles, s);
+    const int dyn = PS_TILE * 10;
+    static bool attr[16] = {};
+    if (!attr[dev().device]) {
+        GX_CUDA(cudaFuncSetAttribute(k_part_scatter<KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+        attr[dev().device] = true;
+    }
+    GX_PROF("partition_scatter", s);
+    k_part_scatter<KW><<<(unsigned)ntiles, PS_NT, dyn, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc);
+    GX_LAUNCHED();
+}
+
+}  // namespace
+
+void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hint, bool gfur, cudaStream_t s,
+                       gx_table* out) {
+    owned_col widened;
+    col key = key_in;
+    if (size_of(key.type) < 4) {
+        widened = widen_to_32(key, s);
+        key.data = widened.buf.get();
+        key.type = widened.type;
+    }
+    const int64_t n = key.n;
+    const int kw = size_of(key.type);
+    const int kind = vkind_of(key.type);
+    const agg_desc& d = p.d;
+    // Shared table: 1 CTA per SM with ~200 KB.
+    size_t per_slot = 8 + 4 + 8 * (size_t)d.n_acc;
+    uint32_t S = 1u << 14;
+    while (S > 256 && S * per_slot > 200 * 1024) S >>= 1;
+    int64_t bound = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
+    if (!(hint->groups_upper_bound > 0 && hint->groups_upper_bound < n) && n > (1 << 16))
+        bound = std::min<int64_t>(n, ndv_estimate(key, s) * 9 / 8 + 64);
+    int R = hint->radix_bits;
+    if (R <= 0) {
+        int64_t per_part = std::max<int64_t>(1, (int64_t)S / 2);
+        R = ilog2_ceil((uint64_t)std::max<int64_t>(1, ceil_div(bound, per_part)));
+        R = std::max(1, std::min(16, R));
+    }
+    R = std::max(1, std::min(16, R));
+    hint->radix_bits = R;
+    const int P = 1 << R;
+
+    // Partitioned copies.
+    move_cols mc;
+    std::memset(&mc, 0, sizeof(mc));
+    std::vector<dbuf> bufs_a, bufs_b;
+    auto add_col = [&](const void* in, int w, int iota) {
+        int c = mc.n++;
+        mc.in[c] = in;
+        mc.width[c] = w;
+        mc.iota[c] = iota;
+        bufs_a.emplace_back((size_t)std::max<int64_t>(n, 1) * w, s);
+        mc.out[c] = bufs_a.back().get();
+    };
+    // 1- and 2-byte value columns are read through row ids (GFUR) instead of
+    // being moved by the 4/8-byte scatter.
+    for (int c = 0; c < d.n_cols; ++c) gfur = gfur || d.col_width[c] < 4;
+    add_col(key.data, kw, 0);
+    if (gfur) add_col(nullptr, 8, 1);
+    else
+        for (int c = 0; c < d.n_cols; ++c) add_col(d.col_ptr[c], d.col_width[c], 0);
+
+    int64_t ntiles = ceil_div(std::max<int64_t>(n, 1), PS_TILE);
+    dbuf counts((size_t)PS_BINS * ntiles * 8, s), offs((size_t)PS_BINS * ntiles * 8 + 8, s);
+    int passes = (R + 7) / 8;
+    // Two digit passes ping-pong between bufs_a and bufs_b.
+    if (passes == 2)
+        for (int c = 0; c < mc.n; ++c) bufs_b.emplace_back((size_t)std::max<int64_t>(n, 1) * mc.width[c], s);
+    if (n > 0) {
+        int shift = 0;
+        for (int ps = 0; ps < passes; ++ps) {
+            int dbits = std::min(8, R - shift);
+            move_cols m = mc;
+            if (passes == 2 && ps == 0) {
+                for (int c = 0; c < mc.n; ++c) m.out[c] = bufs_b[c].get();
+            } else if (passes == 2 && ps == 1) {
+                for (int c = 0; c < mc.n; ++c) { m.in[c] = bufs_b[c].get(); m.iota[c] = 0; m.out[c] = bufs_a[c].get(); }
+            }
+            const void* kin = m.in[0];
+            if (kw == 4) part_pass<4>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), s);
+            else part_pass<8>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), s);
+            shift += dbits;
+        }
+    }
+    // Partition starts: the keys are now grouped by partition id, so
+    // part_start[p] is the first row whose id is >= p.
+    dbuf pstart((size_t)(P + 1) * 8, s);
+    partition_starts(mc.out[0], kw, n, kind, R, pstart.get<int64_t>(), s);
+
+    // Work units.
+    int64_t T = std::max<int64_t>(1 << 14, ceil_div(n, (int64_t)dev().sm_count * 8));
+    dbuf ucount((size_t)P * 8, s), uoff((size_t)(P + 1) * 8, s);
+    k_unit_counts<<<(unsigned)ceil_div(P, 256), 256, 0, s>>>(pstart.get<int64_t>(), P, T, ucount.get<int64_t>());
+    GX_LAUNCHED();
+    exclusive_scan_i64(ucount.get<int64_t>(), uoff.get<int64_t>(), P, s);
+    int64_t max_units = P + ceil_div(n, T) + 1;
+    dbuf units((size_t)max_units * sizeof(unit), s);
+    k_unit_fill<<<(unsigned)ceil_div(P, 256), 256, 0, s>>>(pstart.get<int64_t>(), uoff.get<int64_t>(), P, T,
+                                                           units.get<unit>());
+    GX_LAUNCHED();
+
+    uint64_t empty = kw == 4 ? PG_EMPTY4 : PG_EMPTY8;
+    uint64_t gcap = 1u << 16;
+    int64_t out_cap = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        dbuf grec((gcap + 1) * d.rec_words * 8, s);
+        dbuf flags(16, s);
+        GX_CUDA(cudaMemsetAsync(flags.get(), 0, 16, s));
+        init_records(grec.get<uint64_t>(), (int64_t)gcap + 1, d, empty, s);
+        // Dense output records: at most n groups.
+        dbuf orec((size_t)std::max<int64_t>(n, 1) * d.rec_words * 8, s);
+        unsigned long long* ocount = reinterpret_cast<unsigned long long*>(flags.get<char>() + 8);
+        pglobal g{grec.get<uint64_t>(), gcap - 1, flags.get<int>(), flags.get<int>() + 1};
+        if (n > 0) {
+            size_t smem = (size_t)S * per_slot;
+            int grid = dev().sm_count;
+            move_cols pv;
+            std::memset(&pv, 0, sizeof(pv));
+            if (!gfur)
+                for (int c = 0; c + 1 < mc.n; ++c) pv.out[c] = mc.out[c + 1];
+            const int64_t* prow = gfur ? static_cast<const int64_t*>(mc.out[1]) : nullptr;
+            GX_PROF("partition_aggregate", s);
+            if (kw == 4) {
+                GX_CUDA(cudaFuncSetAttribute(k_part_agg<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                k_part_agg<4><<<grid, PA_NT, smem, s>>>(mc.out[0], prow, pv, kind, d, units.get<unit>(),
+                                                       uoff.get<int64_t>() + P, S, R, g, orec.get<uint64_t>(), ocount);
+            } else {
+                GX_CUDA(cudaFuncSetAttribute(k_part_agg<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                k_part_agg<8><<<grid, PA_NT, smem, s>>>(mc.out[0], prow, pv, kind, d, units.get<unit>(),
+                                                       uoff.get<int64_t>() + P, S, R, g, orec.get<uint64_t>(), ocount);
+            }
+            GX_LAUNCHED();
+        }
+        int ovf = read_scalar(flags.get<int>() + 1, s);
+        if (ovf) { gcap *= 8; continue; }
+        k_append_global<<<grid_for((int64_t)gcap + 1, 256, 4), 256, 0, s>>>(grec.get<uint64_t>(), (int64_t)gcap,
+                                                                          d.rec_words, empty, flags.get<int>(),
+                                                                          orec.get<uint64_t>(), ocount);
+        GX_LAUNCHED();
+        int64_t groups = (int64_t)read_scalar(ocount, s);
+        emit_groupby_output(p, orec.get<uint64_t>(), groups, false, 0, -1, nullptr, key_in.type, out_cap, s, out);
+        return;
+    }
+    fail(GX_EOVERFLOW, "partition group-by spill table overflow after retries");
+}
+
+namespace {
+template <int KW>
+__global__ void k_part_starts(const void* __restrict__ keys, int64_t n, int kind, int R, int64_t* __restrict__ ps, int P) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x) {
+        int cur = i < n ? (int)(part_hash<KW>(ld_key<KW>(keys, i, kind)) & (P - 1)) : P;
+        int prev = i > 0 ? (int)(part_hash<KW>(ld_key<KW>(keys, i - 1, kind)) & (P - 1)) : -1;
+        for (int p = prev + 1; p <= cur; ++p) ps[p] = i;
+    }
+}
+}  // namespace
+
+void partition_starts(const void* keys, int kw, int64_t n, int kind, int R, int64_t* ps, cudaStream_t s) {
+    int P = 1 << R;
+    if (kw == 4) k_part_starts<4><<<grid_for(n + 1, 256, 8), 256, 0, s>>>(keys, n, kind, R, ps, P);
+    else k_part_starts<8><<<grid_for(n + 1, 256, 8), 256, 0, s>>>(keys, n, kind, R, ps, P);
+    GX_LAUNCHED();
+}
+
+}  // namespace gx

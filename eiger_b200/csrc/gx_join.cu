@@ -1,0 +1,350 @@
+// gx_join.cu — sort-based inner equi-join.
+//
+// Replaces gamax::join::inner_eq_join for join_algo SORT
+// (src/cuda/operators/join/inner_join.cu:206-229, sort_merge_join.cu:111-293,
+// merge_path.cuh:22-309).  The reference sorts both sides with CUB, matches
+// them with a merge-path kernel that appends to a circular buffer through a
+// global atomic (nondeterministic order, silent wrap past the allocation)
+// and synchronises on the default stream.
+//
+// B200 design (GX_JOIN_SORTED_BUILD, the default):
+//   1. the smaller side ("build") is radix-sorted on the bits its keys span,
+//      together with its payload (one payload column) or its row id;
+//   2. a radix directory over the sorted run maps the top D bits of a key's
+//      image to the run's bucket, so the sorted run + directory (≈ 96 MB for
+//      2^24 int32 keys) stay L2-resident;
+//   3. the other side ("probe") is streamed once in its stored order: a
+//      count kernel sizes every tile's output exactly, an exclusive scan
+//      places the tiles, and a write kernel emits every (build, probe) pair
+//      in probe order — deterministic, no wrap, no atomics.
+// GX_JOIN_SORT_MERGE sorts the probe side too (key + row id) and runs the
+// same matcher over the sorted stream: the reference's sort-both-sides
+// structure, kept for comparison.
+#include <algorithm>
+
+#include "gx_groupby.h"
+
+namespace gx {
+
+void radix_sort_biased(const col& keys_c, const void* vals_in, int val_width, bool vals_iota,
+                       int begin_bit, int end_bit, bool descending, uint64_t bias, void* keys_out,
+                       void* vals_out, void* temp, size_t temp_bytes, cudaStream_t s);
+
+namespace {
+
+constexpr int JP_NT = 256;
+constexpr int JP_IPT = 8;
+constexpr int JP_TILE = JP_NT * JP_IPT;
+constexpr int MAX_PAY = 8;
+
+template <int KW>
+__device__ __forceinline__ uint64_t img_of(const void* p, int64_t i, int kind) {
+    if (KW == 4) return ordered32(__ldg(static_cast<const unsigned*>(p) + i), kind);
+    return ordered64(__ldg(static_cast<const unsigned long long*>(p) + i), kind);
+}
+
+struct build_run {
+    const void* keys;      // sorted build keys (raw)
+    const void* vals;      // sorted build payload (or row ids)
+    int val_width;         // 4 / 8
+    const uint32_t* dir;   // 2^D + 1 bucket starts
+    int64_t n;
+    uint64_t lo, hi;       // image range of build keys
+    int shift;             // bucket = (img - lo) >> shift
+    int kind;
+};
+
+// First build position with image >= img, and the end of its equal run.
+template <int KW>
+__device__ __forceinline__ void find_run(const build_run& b, uint64_t img, int64_t* first, int64_t* last) {
+    *first = 0;
+    *last = 0;
+    if (img < b.lo || img > b.hi) return;
+    uint64_t bk = (img - b.lo) >> b.shift;
+    int64_t lo = b.dir[bk], hi = b.dir[bk + 1];
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (img_of<KW>(b.keys, mid, b.kind) < img) lo = mid + 1;
+        else hi = mid;
+    }
+    int64_t e = lo;
+    while (e < b.n && img_of<KW>(b.keys, e, b.kind) == img) ++e;
+    *first = lo;
+    *last = e;
+}
+
+struct probe_side {
+    const void* keys;     // probe keys in stream order
+    const int64_t* rowid; // SORT_MERGE: probe row id of stream position (else null)
+    int64_t n;
+    int kind;
+};
+
+template <int KW>
+__global__ void __launch_bounds__(JP_NT) k_probe_count(build_run b, probe_side p, int64_t* __restrict__ tile_out) {
+    int64_t base = blockIdx.x * (int64_t)JP_TILE;
+    int64_t c = 0;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) {
+        int64_t i = base + k * JP_NT + threadIdx.x;
+        if (i < p.n) {
+            int64_t f, l;
+            find_run<KW>(b, img_of<KW>(p.keys, i, p.kind), &f, &l);
+            c += l - f;
+        }
+    }
+    __shared__ int64_t sm[JP_NT / 32];
+    c = dev_::warp_sum(c);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t t = 0;
+        for (int j = 0; j < JP_NT / 32; ++j) t += sm[j];
+        tile_out[blockIdx.x] = t;
+    }
+}
+
+struct join_out {
+    // Output columns: key, then `n_build_pay` build payloads, then `n_probe_pay`.
+    void* key;              // may be null (row-id form)
+    int key_width;
+    int n_pay;              // total payload outputs
+    void* out[2 * MAX_PAY + 2];
+    int width[2 * MAX_PAY + 2];
+    // source: 0 = build run value (sorted payload / row id), 1 = build column
+    // gathered by build row id, 2 = probe column at probe row, 3 = build row id,
+    // 4 = probe row id
+    int src[2 * MAX_PAY + 2];
+    const void* col[2 * MAX_PAY + 2];
+};
+
+__device__ __forceinline__ uint64_t ld_w(const void* p, int w, int64_t i) {
+    switch (w) {
+        case 8: return __ldg(static_cast<const unsigned long long*>(p) + i);
+        case 4: return __ldg(static_cast<const unsigned*>(p) + i);
+        case 2: return static_cast<const uint16_t*>(p)[i];
+        default: return static_cast<const uint8_t*>(p)[i];
+    }
+}
+__device__ __forceinline__ void st_w(void* p, int w, int64_t i, uint64_t v) {
+    switch (w) {
+        case 8: static_cast<unsigned long long*>(p)[i] = v; break;
+        case 4: static_cast<unsigned*>(p)[i] = (unsigned)v; break;
+        case 2: static_cast<uint16_t*>(p)[i] = (uint16_t)v; break;
+        default: static_cast<uint8_t*>(p)[i] = (uint8_t)v; break;
+    }
+}
+
+template <int KW>
+__global__ void __launch_bounds__(JP_NT) k_probe_write(build_run b, probe_side p, const int64_t* __restrict__ tile_off,
+                                                        join_out o) {
+    __shared__ int64_t sm[JP_NT / 32 + 1];
+    // Blocked arrangement: thread t owns rows base + t*IPT .. +IPT so the
+    // output order equals the probe order.
+    int64_t base = blockIdx.x * (int64_t)JP_TILE + threadIdx.x * (int64_t)JP_IPT;
+    int64_t f[JP_IPT], l[JP_IPT];
+    int64_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) {
+        int64_t i = base + k;
+        f[k] = l[k] = 0;
+        if (i < p.n) find_run<KW>(b, img_of<KW>(p.keys, i, p.kind), &f[k], &l[k]);
+        mine += l[k] - f[k];
+    }
+    int64_t total;
+    int64_t pos = tile_off[blockIdx.x] + dev_::block_exclusive_sum<JP_NT, int64_t>(mine, sm, &total);
+    for (int k = 0; k < JP_IPT; ++k) {
+        int64_t i = base + k;
+        for (int64_t m = f[k]; m < l[k]; ++m, ++pos) {
+            int64_t prow = p.rowid ? p.rowid[i] : i;
+            if (o.key) st_w(o.key, o.key_width, pos, ld_w(b.keys, o.key_width, m));
+            for (int c = 0; c < o.n_pay; ++c) {
+                uint64_t v;
+                switch (o.src[c]) {
+                    case 0: v = ld_w(b.vals, b.val_width, m); break;
+                    case 1: v = ld_w(o.col[c], o.width[c], (int64_t)ld_w(b.vals, 8, m)); break;
+                    case 2: v = ld_w(o.col[c], o.width[c], prow); break;
+                    case 3: v = ld_w(b.vals, 8, m); break;
+                    default: v = (uint64_t)prow; break;
+                }
+                st_w(o.out[c], o.width[c], pos, v);
+            }
+        }
+    }
+}
+
+template <int KW>
+__global__ void k_build_dir(const void* __restrict__ skeys, int64_t n, int kind, uint64_t lo, int shift,
+                            uint64_t nb, uint32_t* __restrict__ dir) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t cur = i < n ? (img_of<KW>(skeys, i, kind) - lo) >> shift : nb;
+        uint64_t prev = i > 0 ? (img_of<KW>(skeys, i - 1, kind) - lo) >> shift : (uint64_t)-1;
+        for (uint64_t j = prev + 1; j <= cur; ++j) dir[j] = (uint32_t)i;
+    }
+}
+
+struct sorted_side {
+    dbuf keys, vals;
+    int val_width = 8;
+    bool vals_are_payload = false;
+};
+
+}  // namespace
+
+struct join_inputs {
+    col lkey, rkey;
+    std::vector<col> lpay, rpay;
+};
+
+// Core: returns owned output columns in order [key?, left payloads.., right payloads..]
+// or [left_rowid, right_rowid] when rowids_only.
+static void join_core(const join_inputs& in, const gx_join_hint& hint, bool rowids_only, cudaStream_t s,
+                      gx_table* out) {
+    const int kw = size_of(in.lkey.type);
+    require(in.lkey.type == in.rkey.type, "Join columns cannot have different types");
+    require(kw == 4 || kw == 8, "join: 4- or 8-byte key columns supported");
+    const int kind = vkind_of(in.lkey.type);
+    // Build = smaller side.
+    bool build_left = in.lkey.n <= in.rkey.n;
+    const col& bkey = build_left ? in.lkey : in.rkey;
+    const col& pkey = build_left ? in.rkey : in.lkey;
+    const std::vector<col>& bpay = build_left ? in.lpay : in.rpay;
+    const std::vector<col>& ppay = build_left ? in.rpay : in.lpay;
+    require((int)bpay.size() <= MAX_PAY && (int)ppay.size() <= MAX_PAY, "join: too many payload columns");
+
+    const int64_t nb = bkey.n, np = pkey.n;
+    // Sort the build side: (key, payload) when exactly one 4/8-byte payload.
+    bool pay_in_run = !rowids_only && bpay.size() == 1 && (size_of(bpay[0].type) == 4 || size_of(bpay[0].type) == 8);
+    int vw = pay_in_run ? size_of(bpay[0].type) : 8;
+    dbuf bk((size_t)std::max<int64_t>(nb, 1) * kw, s), bv((size_t)std::max<int64_t>(nb, 1) * vw, s);
+    uint64_t lo = 0, hi = 0;
+    if (nb > 0) key_image_range(bkey, &lo, &hi, s);
+    uint64_t span = hi - lo;
+    int nbits = span == 0 ? 1 : 64 - __builtin_clzll(span);
+    if (nb > 0) {
+        if (pay_in_run) radix_sort_biased(bkey, bpay[0].data, vw, false, 0, nbits, false, lo, bk.get(), bv.get(), nullptr, 0, s);
+        else radix_sort_biased(bkey, nullptr, 8, true, 0, nbits, false, lo, bk.get(), bv.get(), nullptr, 0, s);
+    }
+    // Directory: D bits, about two build keys per bucket.
+    int D = std::min(nbits, std::max(1, ilog2_ceil((uint64_t)std::max<int64_t>(nb, 2)) - 1));
+    int shift = nbits - D;
+    uint64_t nbk = (span >> shift) + 1;
+    dbuf dir((size_t)(nbk + 1) * 4, s);
+    if (nb > 0) {
+        if (kw == 4) k_build_dir<4><<<grid_for(nb + 1, 256, 8), 256, 0, s>>>(bk.get(), nb, kind, lo, shift, nbk, dir.get<uint32_t>());
+        else k_build_dir<8><<<grid_for(nb + 1, 256, 8), 256, 0, s>>>(bk.get(), nb, kind, lo, shift, nbk, dir.get<uint32_t>());
+        GX_LAUNCHED();
+    }
+    build_run br{bk.get(), bv.get(), vw, dir.get<uint32_t>(), nb, lo, hi, shift, kind};
+
+    // Probe stream (sorted for SORT_MERGE).
+    probe_side ps{pkey.data, nullptr, np, kind};
+    dbuf psk, psr;
+    if (hint.sort_mode == GX_JOIN_SORT_MERGE && np > 0) {
+        uint64_t plo, phi;
+        key_image_range(pkey, &plo, &phi, s);
+        uint64_t pspan = phi - plo;
+        int pbits = pspan == 0 ? 1 : 64 - __builtin_clzll(pspan);
+        psk = dbuf((size_t)np * kw, s);
+        psr = dbuf((size_t)np * 8, s);
+        radix_sort_biased(pkey, nullptr, 8, true, 0, pbits, false, plo, psk.get(), psr.get(), nullptr, 0, s);
+        ps.keys = psk.get();
+        ps.rowid = psr.get<int64_t>();
+    }
+
+    int64_t ntiles = ceil_div(std::max<int64_t>(np, 1), JP_TILE);
+    dbuf tc(ntiles * 8, s), toff((ntiles + 1) * 8, s);
+    int64_t total = 0;
+    if (np > 0 && nb > 0) {
+        GX_PROF("join_probe_count", s);
+        if (kw == 4) k_probe_count<4><<<(unsigned)ntiles, JP_NT, 0, s>>>(br, ps, tc.get<int64_t>());
+        else k_probe_count<8><<<(unsigned)ntiles, JP_NT, 0, s>>>(br, ps, tc.get<int64_t>());
+        GX_LAUNCHED();
+        exclusive_scan_i64(tc.get<int64_t>(), toff.get<int64_t>(), ntiles, s);
+        total = read_scalar(toff.get<int64_t>() + ntiles, s);
+    }
+    if (hint.max_out > 0 && total > hint.max_out)
+        fail(GX_EOVERFLOW, "join output (" + std::to_string(total) + " rows) exceeds hint.max_out (" +
+                               std::to_string(hint.max_out) + ")");
+
+    join_out o;
+    std::memset(&o, 0, sizeof(o));
+    out->cols.clear();
+    if (rowids_only) {
+        out->cols.push_back(make_col(GX_INT64, total, s));
+        out->cols.push_back(make_col(GX_INT64, total, s));
+        o.n_pay = 2;
+        // left row id, right row id
+        o.out[0] = out->cols[0].buf.get(); o.width[0] = 8; o.src[0] = build_left ? 3 : 4;
+        o.out[1] = out->cols[1].buf.get(); o.width[1] = 8; o.src[1] = build_left ? 4 : 3;
+    } else {
+        out->cols.push_back(make_col(in.lkey.type, total, s));
+        o.key = out->cols[0].buf.get();
+        o.key_width = kw;
+        auto add_side = [&](bool is_build, const std::vector<col>& pays) {
+            for (size_t c = 0; c < pays.size(); ++c) {
+                int w = size_of(pays[c].type);
+                require(w > 0, "join: STRING payload columns are not supported");
+                out->cols.push_back(make_col(pays[c].type, total, s));
+                int j = o.n_pay++;
+                o.out[j] = out->cols.back().buf.get();
+                o.width[j] = w;
+                o.col[j] = pays[c].data;
+                o.src[j] = is_build ? (pay_in_run ? 0 : 1) : 2;
+            }
+        };
+        // Output order is always [key, left payloads, right payloads].
+        if (build_left) { add_side(true, in.lpay); add_side(false, in.rpay); }
+        else { add_side(false, in.lpay); add_side(true, in.rpay); }
+    }
+    if (total > 0) {
+        GX_PROF("join_probe_write", s);
+        if (kw == 4) k_probe_write<4><<<(unsigned)ntiles, JP_NT, 0, s>>>(br, ps, toff.get<int64_t>(), o);
+        else k_probe_write<8><<<(unsigned)ntiles, JP_NT, 0, s>>>(br, ps, toff.get<int64_t>(), o);
+        GX_LAUNCHED();
+    }
+    GX_CUDA(cudaStreamSynchronize(s));
+}
+
+void inner_eq_join(const gx_table_view* left, const gx_table_view* right, const gx_join_hint* hint,
+                   cudaStream_t s, gx_table* out) {
+    require(left && right && hint, "join: null argument");
+    // Validation mirrors check_join_solvable (inner_join.cu:17-45).
+    if (hint->join_algo == GX_JOIN_AUTO || hint->mat_algo == GX_MAT_AUTO)
+        fail(GX_EINVAL, "Join algorithm and materialization algorithm do not support auto selection");
+    if (hint->max_out > GX_MAX_JOIN_OUTPUT_SIZE) fail(GX_EINVAL, "Output size exceeds the maximum limit");
+    if (hint->mat_algo == GX_MAT_INDEX_CLUSTER)
+        fail(GX_EINVAL, "Index cluster materialization algorithm is not supported");
+    if (left->num_columns == 0 || right->num_columns == 0) fail(GX_EINVAL, "Empty table");
+    if (left->columns[0].type != right->columns[0].type) fail(GX_EINVAL, "Join columns cannot have different types");
+    if (left->num_columns == 1 || right->num_columns == 1)
+        fail(GX_EINVAL, "Left and right table should have at least 1 payload column");
+    if (hint->join_algo != GX_JOIN_SORT)
+        fail(GX_EUNSUPPORTED, "only join_algo SORT is implemented by this library");
+    join_inputs in;
+    in.lkey = resolve(left->columns[0]);
+    in.rkey = resolve(right->columns[0]);
+    for (int64_t c = 1; c < left->num_columns; ++c) {
+        in.lpay.push_back(resolve(left->columns[c]));
+        require(in.lpay.back().n == in.lkey.n, "join: left payload length differs from key length");
+    }
+    for (int64_t c = 1; c < right->num_columns; ++c) {
+        in.rpay.push_back(resolve(right->columns[c]));
+        require(in.rpay.back().n == in.rkey.n, "join: right payload length differs from key length");
+    }
+    join_core(in, *hint, false, s, out);
+}
+
+void inner_eq_join_rowids(const gx_column_view& l, const gx_column_view& r, const gx_join_hint* hint,
+                          cudaStream_t s, gx_table* out) {
+    join_inputs in;
+    in.lkey = resolve(l);
+    in.rkey = resolve(r);
+    gx_join_hint h;
+    if (hint) h = *hint;
+    else { std::memset(&h, 0, sizeof(h)); h.join_algo = GX_JOIN_SORT; h.mat_algo = GX_MAT_GFUR; }
+    if (h.max_out > GX_MAX_JOIN_OUTPUT_SIZE) fail(GX_EINVAL, "Output size exceeds the maximum limit");
+    join_core(in, h, true, s, out);
+}
+
+}  // namespace gx

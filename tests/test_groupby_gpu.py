@@ -1,0 +1,188 @@
+"""Group-by parity: the CUDA library (through its C ABI) against the CPU
+oracle, for every variant (HASH, SORT, SORT_OPT, SORT_GFUR, PARTITION,
+PARTITION_GFUR, AUTO), key/value dtypes, aggregations and key
+distributions, plus the edge cases the reference's tests cover.  Integer
+results are compared bit-exact after sorting by key; float64 SUM / AVG
+within 1e-12 relative."""
+import numpy as np
+import pytest
+
+import eiger_b200 as gx
+import oracle as O
+from tests.helpers import assert_columns_match, sort_by_key, to_dev
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = [gx.HASH, gx.SORT, gx.SORT_OPT, gx.SORT_GFUR, gx.PARTITION, gx.PARTITION_GFUR]
+OKIND = {gx.SUM: O.SUM, gx.MIN: O.MIN, gx.MAX: O.MAX, gx.AVG: O.AVG, gx.ANY: O.ANY, gx.COUNT_ALL: O.COUNT_ALL}
+
+
+def run_both(key, vals, reqs, algo, bound=None, agg_count=False, **hint_kw):
+    hint = gx.make_hint(algo, bound, agg_count=int(agg_count), **hint_kw)
+    t = gx.groupby([to_dev(key)], [to_dev(v) for v in vals], reqs, hint)
+    got = sort_by_key(t.numpy_columns())
+    exp = O.groupby(key, vals, [(c, OKIND[k]) for c, k in reqs], agg_count=agg_count)
+    return got, exp, hint
+
+
+@pytest.mark.parametrize("algo", VARIANTS)
+def test_c1_hash_groupby_config(algo):
+    # 2^20 rows, int32 keys uniform over 1024 values, int64 values in [0, 1e6), SUM + COUNT.
+    n = 1 << 20
+    key = O.gen_keys(n, np.int32, groups=1024, seed=42, stream_id=0)
+    val = O.gen_values(n, np.int64, lo=0, hi=1_000_000, seed=42, stream_id=1)
+    got, exp, _ = run_both(key, [val], [(0, gx.SUM), (0, gx.COUNT_ALL)], algo, bound=1024)
+    assert_columns_match(got, exp)
+
+
+@pytest.mark.parametrize("algo", VARIANTS)
+@pytest.mark.parametrize("kdt", [np.int32, np.int64])
+@pytest.mark.parametrize("G,dist,s", [(16, O.DIST_UNIFORM, 0.0), (5000, O.DIST_UNIFORM, 0.0),
+                                      (1 << 17, O.DIST_UNIFORM, 0.0), (4096, O.DIST_ZIPF, 1.0),
+                                      (1 << 16, O.DIST_ZIPF, 1.5)])
+def test_sweep_all_aggregates(algo, kdt, G, dist, s):
+    n = 1 << 18
+    key = O.gen_keys(n, kdt, dist=dist, groups=G, zipf_s=s, scatter=1, seed=5)
+    iv = O.gen_values(n, np.int64, lo=0, hi=1 << 31, seed=6)
+    fv = O.gen_values(n, np.float64, seed=7)
+    reqs = [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
+    got, exp, hint = run_both(key, [iv, fv], reqs, algo, bound=G)
+    assert_columns_match(got, exp)
+    assert hint.groupby_algo == (gx.SORT_OPT if algo == gx.SORT_OPT else algo)
+
+
+@pytest.mark.parametrize("algo", VARIANTS)
+def test_unknown_bound_high_cardinality(algo):
+    # No groups_upper_bound: the engine sizes its tables itself.
+    n = 1 << 18
+    key = O.gen_keys(n, np.int32, groups=1 << 17, scatter=1, seed=8)
+    val = O.gen_values(n, np.int64, lo=-100, hi=100, seed=9)
+    got, exp, _ = run_both(key, [val], [(0, gx.SUM), (0, gx.MAX)], algo)
+    assert_columns_match(got, exp)
+
+
+@pytest.mark.parametrize("algo", VARIANTS)
+@pytest.mark.parametrize("vdt", [np.int8, np.int16, np.int32, np.uint32, np.float32, np.int64, np.float64])
+def test_value_types(algo, vdt):
+    n = 20000
+    key = O.gen_keys(n, np.int64, groups=300, scatter=1, seed=10)
+    if np.dtype(vdt).kind == "f":
+        val = (O.gen_values(n, np.float64, seed=11) * 200 - 100).astype(vdt)
+    else:
+        info = np.iinfo(vdt)
+        val = O.gen_values(n, np.int64, lo=max(info.min, -(1 << 30)), hi=min(info.max, 1 << 30), seed=11).astype(vdt)
+    reqs = [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (0, gx.AVG)]
+    got, exp, _ = run_both(key, [val], reqs, algo, bound=300)
+    assert_columns_match(got, exp)
+
+
+@pytest.mark.parametrize("algo", VARIANTS)
+@pytest.mark.parametrize("kdt", [np.int8, np.int16, np.uint32, np.uint64, np.float32, np.float64])
+def test_key_types(algo, kdt):
+    n = 30000
+    if np.dtype(kdt).kind == "f":
+        key = (O.gen_keys(n, np.int64, groups=200, seed=12).astype(np.float64) - 100).astype(kdt) * kdt(0.5)
+    else:
+        key = O.gen_keys(n, np.int64, groups=120, seed=12).astype(kdt)
+    val = O.gen_values(n, np.int64, lo=0, hi=1000, seed=13)
+    got, exp, _ = run_both(key, [val], [(0, gx.SUM), (0, gx.COUNT_ALL)], algo)
+    assert_columns_match(got, exp)
+
+
+@pytest.mark.parametrize("algo", VARIANTS)
+def test_edge_cases(algo):
+    cases = {
+        "one_row": np.array([7], dtype=np.int64),
+        "single_group": np.full(10000, -3, dtype=np.int64),
+        "all_unique": np.arange(50000, dtype=np.int64)[::-1].copy(),
+        "negative": np.array([-1, -2, -1, 5, -2, 5, 0], dtype=np.int64),
+        "sentinel_keys": np.array([np.iinfo(np.int64).min, 0, np.iinfo(np.int64).min, -1, np.iinfo(np.int64).max],
+                                  dtype=np.int64),
+        "int32_extremes": np.array([np.iinfo(np.int32).min, -1, np.iinfo(np.int32).max, -1], dtype=np.int32),
+    }
+    for name, key in cases.items():
+        val = np.arange(len(key), dtype=np.int64) * 3 - 7
+        got, exp, _ = run_both(key, [val], [(0, gx.SUM), (0, gx.MIN), (0, gx.COUNT_ALL)], algo)
+        assert_columns_match(got, exp)
+
+
+@pytest.mark.parametrize("algo", VARIANTS)
+def test_empty_input(algo):
+    key = np.zeros(0, dtype=np.int32)
+    val = np.zeros(0, dtype=np.int64)
+    import torch
+    hint = gx.make_hint(algo)
+    t = gx.groupby([torch.zeros(0, dtype=torch.int32, device="cuda")],
+                   [torch.zeros(0, dtype=torch.int64, device="cuda")], [(0, gx.SUM)], hint)
+    assert t.num_rows == 0 and t.num_columns == 2
+    assert t.type(1) == gx.INT64
+
+
+def test_float_zero_keys_merge():
+    key = np.array([0.0, -0.0, 1.5, -0.0, 1.5], dtype=np.float64)
+    val = np.arange(5, dtype=np.int64)
+    for algo in VARIANTS:
+        got, exp, _ = run_both(key, [val], [(0, gx.SUM)], algo)
+        assert len(got[0]) == 2
+        assert np.array_equal(got[1], exp[1])
+
+
+def test_agg_count_hint_and_avg_layout():
+    # Output layout follows groupby.cu:346-392: [key, requests..., count].
+    key = np.array([1, 1, 2, 2, 2], dtype=np.int32)
+    val = np.array([10, 20, 30, 40, 50], dtype=np.int32)
+    for algo in VARIANTS:
+        got, exp, _ = run_both(key, [val], [(0, gx.AVG), (0, gx.SUM)], algo, agg_count=True)
+        assert [g.dtype for g in got] == [np.int32, np.float64, np.int64, np.int64]
+        assert_columns_match(got, exp)
+
+
+def test_auto_heuristic_choice():
+    # groupby.cu:99-118: NDV <= 2^14 (4-byte keys) -> HASH, else PARTITION.
+    n = 1 << 18
+    low = O.gen_keys(n, np.int32, groups=1000, seed=1)
+    high = O.gen_keys(n, np.int32, groups=1 << 17, scatter=1, seed=1)
+    val = np.ones(n, dtype=np.int64)
+    for key, want in ((low, gx.HASH), (high, gx.PARTITION)):
+        hint = gx.make_hint(gx.AUTO_ALGO)
+        gx.groupby([to_dev(key)], [to_dev(val)], [(0, gx.SUM)], hint)
+        assert hint.groupby_algo == want
+
+
+def test_any_returns_a_group_member():
+    n = 10000
+    key = O.gen_keys(n, np.int32, groups=50, seed=3)
+    val = O.gen_values(n, np.int64, lo=0, hi=1 << 40, seed=4)
+    for algo in VARIANTS:
+        t = gx.groupby([to_dev(key)], [to_dev(val)], [(0, gx.ANY)], gx.make_hint(algo, 50))
+        k, a = t.numpy_columns()
+        for kk, aa in zip(k, a):
+            assert aa in set(val[key == kk].tolist())
+
+
+def test_partition_radix_bits_and_overflow_spill():
+    # A tiny fan-out forces partitions past their shared-table capacity; the
+    # spill path must still produce exact results (the reference throws).
+    n = 1 << 18
+    key = O.gen_keys(n, np.int64, groups=1 << 16, scatter=1, seed=21)
+    val = O.gen_values(n, np.int64, lo=0, hi=100, seed=22)
+    for bits in (1, 4, 9, 16):
+        got, exp, hint = run_both(key, [val], [(0, gx.SUM), (0, gx.COUNT_ALL)], gx.PARTITION, radix_bits=bits)
+        assert hint.radix_bits == bits
+        assert_columns_match(got, exp)
+
+
+def test_closed_form_uniform_2_28_property():
+    # Full-size property check (groupby_test.hpp:64-74): 2^26 rows of
+    # shuffled i % G keys with all-ones values; every group sums to N/G.
+    import torch
+    n, G = 1 << 26, 1 << 20
+    k = torch.empty(n, dtype=torch.int32, device="cuda")
+    gx.generate_keys(k, gx.gen_spec(seed=1, dist=gx.DIST_CYCLIC, groups=G))
+    ones = torch.ones(n, dtype=torch.int32, device="cuda")
+    for algo in (gx.HASH, gx.PARTITION, gx.SORT):
+        t = gx.groupby([k], [ones, ones], [(0, gx.SUM), (1, gx.SUM)], gx.make_hint(algo, G))
+        keys, s0, s1 = t.numpy_columns()
+        assert len(keys) == G
+        assert np.all(s0 == n // G) and np.all(s1 == n // G)
+        assert int(keys.astype(np.int64).sum()) == G * (G - 1) // 2
