@@ -225,9 +225,11 @@ __global__ void __launch_bounds__(PA_NT) k_part_agg(const void* __restrict__ pke
                                                      int kind, agg_desc d, const unit* __restrict__ units,
                                                      const int64_t* __restrict__ n_units, uint32_t S, int rbits,
                                                      pglobal g, uint64_t* __restrict__ out_recs,
-                                                     unsigned long long* __restrict__ out_count) {
+                                                     unsigned long long* __restrict__ out_count, int64_t rec_cap,
+                                                     int* __restrict__ rec_overflow) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_fill;
+    __shared__ int s_spilled;
     __shared__ unsigned long long s_base;
     unsigned long long* skeys = reinterpret_cast<unsigned long long*>(smem);
     unsigned* scnt = reinterpret_cast<unsigned*>(smem + (size_t)S * 8);
@@ -246,7 +248,7 @@ __global__ void __launch_bounds__(PA_NT) k_part_agg(const void* __restrict__ pke
                          : 0ull;
             for (uint32_t i = threadIdx.x; i < S; i += PA_NT) sacc[(size_t)a * S + i] = idv;
         }
-        if (threadIdx.x == 0) s_fill = 0;
+        if (threadIdx.x == 0) { s_fill = 0; s_spilled = 0; }
         __syncthreads();
         for (int64_t i = un.begin + threadIdx.x; i < un.end; i += PA_NT) {
             uint64_t kw = ld_key<KW>(pkeys, i, kind);
@@ -283,6 +285,7 @@ __global__ void __launch_bounds__(PA_NT) k_part_agg(const void* __restrict__ pke
                 for (int a = 0; a < d.n_acc; ++a)
                     dev_::acc_atomic(sacc + (size_t)a * S + found, d.acc_op[a], d.acc_kind[a], dev_::pick(v, d.acc_col[a]));
             } else {
+                if (!s_spilled) s_spilled = 1;
                 uint64_t* r = pg_find<KW>(g, d, kw, h);
                 if (r) {
                     if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), 1ull);
@@ -292,10 +295,16 @@ __global__ void __launch_bounds__(PA_NT) k_part_agg(const void* __restrict__ pke
             }
         }
         __syncthreads();
-        if (!un.split) {
+        // A unit that spilled may hold a key both here and in the spill table
+        // (a row raced the table closing), so it merges like a split unit.
+        if (!un.split && !s_spilled) {
             // Whole partition in this CTA: its groups are final; append them densely.
-            if (threadIdx.x == 0) s_base = atomicAdd(out_count, (unsigned long long)s_fill);
+            if (threadIdx.x == 0) {
+                s_base = atomicAdd(out_count, (unsigned long long)s_fill);
+                if ((int64_t)(s_base + s_fill) > rec_cap) atomicExch(rec_overflow, 1);
+            }
             __syncthreads();
+            if ((int64_t)(s_base + s_fill) > rec_cap) { __syncthreads(); continue; }
             // Compact occupied slots in slot order with a block scan.
             __shared__ int64_t scan_sm[PA_NT / 32 + 1];
             int64_t running = 0;
@@ -330,12 +339,14 @@ __global__ void __launch_bounds__(PA_NT) k_part_agg(const void* __restrict__ pke
 // Append the occupied records of the global spill table after the dense ones.
 __global__ void k_append_global(const uint64_t* __restrict__ g, int64_t cap, int rec_words, uint64_t empty,
                                 const int* __restrict__ sentinel_flag, uint64_t* __restrict__ out,
-                                unsigned long long* __restrict__ out_count) {
+                                unsigned long long* __restrict__ out_count, int64_t rec_cap,
+                                int* __restrict__ rec_overflow) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r <= cap; r += (int64_t)gridDim.x * blockDim.x) {
         const uint64_t* src = g + r * rec_words;
         bool live = r < cap ? src[0] != empty : *sentinel_flag != 0;
         if (!live) continue;
         unsigned long long pos = atomicAdd(out_count, 1ull);
+        if ((int64_t)pos >= rec_cap) { atomicExch(rec_overflow, 1); continue; }
         for (int w = 0; w < rec_words; ++w) out[pos * rec_words + w] = src[w];
     }
 }
@@ -458,14 +469,16 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     uint64_t empty = kw == 4 ? PG_EMPTY4 : PG_EMPTY8;
     uint64_t gcap = 1u << 16;
     int64_t out_cap = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
-    for (int attempt = 0; attempt < 6; ++attempt) {
+    // Output records: sized from the group bound, grown (up to n) on overflow.
+    int64_t rec_cap = std::max<int64_t>(1, std::min<int64_t>(n, std::max<int64_t>(bound + bound / 4, 4096)));
+    for (int attempt = 0; attempt < 8; ++attempt) {
         dbuf grec((gcap + 1) * d.rec_words * 8, s);
-        dbuf flags(16, s);
-        GX_CUDA(cudaMemsetAsync(flags.get(), 0, 16, s));
+        dbuf flags(32, s);  // [0] sentinel, [1] spill overflow, [8..15] count, [16] record overflow
+        GX_CUDA(cudaMemsetAsync(flags.get(), 0, 32, s));
         init_records(grec.get<uint64_t>(), (int64_t)gcap + 1, d, empty, s);
-        // Dense output records: at most n groups.
-        dbuf orec((size_t)std::max<int64_t>(n, 1) * d.rec_words * 8, s);
+        dbuf orec((size_t)rec_cap * d.rec_words * 8, s);
         unsigned long long* ocount = reinterpret_cast<unsigned long long*>(flags.get<char>() + 8);
+        int* rec_ovf = reinterpret_cast<int*>(flags.get<char>() + 16);
         pglobal g{grec.get<uint64_t>(), gcap - 1, flags.get<int>(), flags.get<int>() + 1};
         if (n > 0) {
             size_t smem = (size_t)S * per_slot;
@@ -479,11 +492,13 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
             if (kw == 4) {
                 GX_CUDA(cudaFuncSetAttribute(k_part_agg<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 k_part_agg<4><<<grid, PA_NT, smem, s>>>(mc.out[0], prow, pv, kind, d, units.get<unit>(),
-                                                       uoff.get<int64_t>() + P, S, R, g, orec.get<uint64_t>(), ocount);
+                                                       uoff.get<int64_t>() + P, S, R, g, orec.get<uint64_t>(), ocount,
+                                                       rec_cap, rec_ovf);
             } else {
                 GX_CUDA(cudaFuncSetAttribute(k_part_agg<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 k_part_agg<8><<<grid, PA_NT, smem, s>>>(mc.out[0], prow, pv, kind, d, units.get<unit>(),
-                                                       uoff.get<int64_t>() + P, S, R, g, orec.get<uint64_t>(), ocount);
+                                                       uoff.get<int64_t>() + P, S, R, g, orec.get<uint64_t>(), ocount,
+                                                       rec_cap, rec_ovf);
             }
             GX_LAUNCHED();
         }
@@ -491,9 +506,14 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
         if (ovf) { gcap *= 8; continue; }
         k_append_global<<<grid_for((int64_t)gcap + 1, 256, 4), 256, 0, s>>>(grec.get<uint64_t>(), (int64_t)gcap,
                                                                           d.rec_words, empty, flags.get<int>(),
-                                                                          orec.get<uint64_t>(), ocount);
+                                                                          orec.get<uint64_t>(), ocount, rec_cap,
+                                                                          rec_ovf);
         GX_LAUNCHED();
         int64_t groups = (int64_t)read_scalar(ocount, s);
+        if (read_scalar(rec_ovf, s)) {
+            rec_cap = std::min<int64_t>(std::max<int64_t>(n, 1), rec_cap * 4);
+            continue;
+        }
         emit_groupby_output(p, orec.get<uint64_t>(), groups, false, 0, -1, nullptr, key_in.type, out_cap, s, out);
         return;
     }

@@ -263,10 +263,11 @@ __global__ void k_narrow(D* __restrict__ out, const S* __restrict__ in, int64_t 
 size_t radix_temp_bytes(int64_t n, int key_width, int val_width) {
     int kw = key_width < 4 ? 4 : key_width;
     int64_t ntiles = ceil_div(std::max<int64_t>(n, 1), RS_TILE);
-    size_t b = (size_t)n * (kw + val_width) + 256;
-    b += (size_t)RS_BINS * ntiles * 8 * 2 + 512;
-    if (key_width < 4) b += (size_t)n * 4 * 2 + 256;
-    return b;
+    // Six sub-buffers, each rounded up to 256 bytes: 6 * 256 of slack.
+    size_t b = (size_t)n * (kw + val_width);
+    b += (size_t)RS_BINS * ntiles * 8 * 2 + 8;
+    if (key_width < 4) b += (size_t)n * 4 * 2;
+    return b + 6 * 256 + 256;
 }
 
 void key_image_range(const col& keys, uint64_t* lo, uint64_t* hi, cudaStream_t s) {
