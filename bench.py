@@ -241,30 +241,34 @@ def run_gx(args) -> None:
         gx.generate_keys(pk, gx.gen_spec(seed=39 + rank, groups=nb, miss_frac=0.1))
         prow = torch.arange(npr, dtype=torch.int64, device="cuda")
         jh = gx.make_join_hint(gx.JOIN_SORT, gx.MAT_GFUR, unique_left=1)
+        nsteps = max(1, args.steps // 2)
 
-        def jstep():
-            return gx.inner_eq_join([bk, brow], [pk, prow], jh)
+        def measure(fn, alg_bytes_of):
+            r = fn()
+            matches = r.num_rows
+            del r
+            gx.lib.gx_profile_reset()
+            gx.lib.gx_profile_enable(1)
+            ms = time_steps(torch, fn, nsteps, 3, dist) / nsteps
+            gx.lib.gx_profile_enable(0)
+            wms, wc = kernel_ms(gx, "join_probe_write")
+            cms, cc = kernel_ms(gx, "join_probe_count")
+            gx.lib.gx_profile_reset()
+            alg = alg_bytes_of(matches)
+            probe_ms = wms / max(wc, 1) + cms / max(cc, 1)
+            return {"value": world * (nb + npr) / (ms * 1e-3) / 1e6, "unit": "Mrows/s", "ms_per_step": ms,
+                    "matches": matches, "probe_write_ms": wms / max(wc, 1), "probe_count_ms": cms / max(cc, 1),
+                    "probe_frac": alg / (probe_ms * 1e-3) / 1e9 / peaks["hbm_gbs"] if wc else None,
+                    "operator_frac": alg / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                    "algorithmic_bytes": alg}
 
-        r = jstep()
-        matches = r.num_rows
-        del r
-        gx.lib.gx_profile_reset()
-        gx.lib.gx_profile_enable(1)
-        jms = time_steps(torch, jstep, max(1, args.steps // 2), 2, dist) / max(1, args.steps // 2)
-        gx.lib.gx_profile_enable(0)
-        wms, wc = kernel_ms(gx, "join_probe_write")
-        cms, cc = kernel_ms(gx, "join_probe_count")
-        gx.lib.gx_profile_reset()
-        probe_bytes = npr * (4 + 8) + matches * (4 + 8 + 8)
-        jalg = (nb + npr) * (4 + 8) + matches * (4 + 8 + 8)
-        join = {"workload": "sort-based inner equi-join, 2^24 unique int32 build keys (int64 payload) x "
-                            f"{npr} int32 probe keys (10% absent, int64 payload)",
-                "value": world * (nb + npr) / (jms * 1e-3) / 1e6, "unit": "Mrows/s", "ms_per_step": jms,
-                "matches": matches,
-                "probe_write_ms": wms / max(wc, 1), "probe_count_ms": cms / max(cc, 1),
-                "probe_frac": probe_bytes / ((wms / max(wc, 1) + cms / max(cc, 1)) * 1e-3) / 1e9 / peaks["hbm_gbs"]
-                if wc else None,
-                "operator_frac": jalg / (jms * 1e-3) / 1e9 / peaks["hbm_gbs"]}
+        # Row-id pairs (build_rowid, probe_rowid): |R|*4 + |S|*4 + M*16 bytes.
+        join = measure(lambda: gx.inner_eq_join_rowids(bk, pk, jh), lambda m: (nb + npr) * 4 + m * 16)
+        join["workload"] = (f"sort-based inner equi-join, 2^24 unique int32 build keys x {npr} int32 probe keys "
+                            "(10% absent); output (build_rowid, probe_rowid) int64 pairs")
+        # Table form [key, build payload, probe payload] with int64 payloads.
+        join["table_form"] = measure(lambda: gx.inner_eq_join([bk, brow], [pk, prow], jh),
+                                     lambda m: (nb + npr) * 12 + m * 20)
         del bk, brow, pk, prow
 
     # ------------------------------------------------------ cpu baseline
@@ -288,6 +292,59 @@ def run_gx(args) -> None:
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_sweep(args) -> None:
+    """Group-by sweep (rows fixed, distinct count and skew swept) over the
+    HASH / SORT / PARTITION variants; one JSON line per point."""
+    import torch
+    import eiger_b200 as gx
+
+    torch.cuda.set_device(0)
+    peaks = measured_peaks()
+    rows = args.rows
+    gs = [int(g) for g in args.sweep_groups.split(",")]
+    zs = [float(z) for z in args.sweep_zipf.split(",")]
+    algos = {"hash": gx.HASH, "sort": gx.SORT, "partition": gx.PARTITION}
+    reqs = groupby_reqs(gx)
+    for kdt in args.sweep_keys.split(","):
+        tdt = torch.int32 if kdt == "int32" else torch.int64
+        for z in zs:
+            for G in gs:
+                k = torch.empty(rows, dtype=tdt, device="cuda")
+                cdf = None
+                if z > 0:
+                    cdf = torch.from_numpy(gx.zipf_cdf(G, z)).cuda()
+                    spec = gx.gen_spec(seed=1, dist=gx.DIST_ZIPF, groups=G, zipf_s=z, scatter=1,
+                                       zipf_cdf=cdf.data_ptr())
+                else:
+                    spec = gx.gen_spec(seed=1, groups=G, scatter=1)
+                gx.generate_keys(k, spec)
+                iv = torch.empty(rows, dtype=torch.int64, device="cuda")
+                gx.generate_values(iv, gx.gen_spec(seed=1, stream_id=1, lo=0, hi=1 << 31))
+                fv = torch.empty(rows, dtype=torch.float64, device="cuda")
+                gx.generate_values(fv, gx.gen_spec(seed=1, stream_id=2))
+                kb = 4 if kdt == "int32" else 8
+                for name in args.sweep_algos.split(","):
+                    algo = algos[name]
+
+                    def step():
+                        return gx.groupby([k], [iv, fv], reqs, gx.make_hint(algo, G))
+                    try:
+                        r = step()
+                        ng = r.num_rows
+                        del r
+                        ms = time_steps(torch, step, args.steps, 2) / args.steps
+                        alg = rows * (kb + 16) + ng * (kb + 56)
+                        print(json.dumps({"key": kdt, "zipf": z, "groups": G, "algo": name, "ms": round(ms, 3),
+                                          "mrows_s": round(rows / ms / 1e3, 1),
+                                          "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4),
+                                          "groups_found": ng}), flush=True)
+                    except Exception as e:  # report and continue the sweep
+                        print(json.dumps({"key": kdt, "zipf": z, "groups": G, "algo": name, "error": str(e)}),
+                              flush=True)
+                del k, iv, fv, cdf
+                torch.cuda.empty_cache()
 
 
 def cpu_groupby_baseline(rows: int, groups: int) -> dict:
@@ -352,9 +409,17 @@ def main() -> None:
     ap.add_argument("--cpu-rows", type=int, default=1 << 24)
     ap.add_argument("--traffic", type=float, default=None,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
+    ap.add_argument("--sweep", action="store_true", help="group-by sweep over variants, groups and skew")
+    ap.add_argument("--sweep-groups", default=",".join(str(1 << b) for b in range(4, 27, 2)))
+    ap.add_argument("--sweep-zipf", default="0")
+    ap.add_argument("--sweep-keys", default="int32")
+    ap.add_argument("--sweep-algos", default="hash,sort,partition")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.sweep:
+        run_sweep(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

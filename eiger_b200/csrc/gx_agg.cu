@@ -117,6 +117,14 @@ agg_plan make_agg_plan(const gx_table_view* val, const gx_agg_request* req, int 
         o.out_type = GX_INT64;
         p.outs.push_back(o);
     }
+    for (int a = 0; a < p.d.n_acc; ++a) {
+        int op = p.d.acc_op[a], kind = p.d.acc_kind[a];
+        int cl = op == OP_SUM ? (kind == VK_F ? CL_FSUM : CL_ISUM) : op == OP_MIN ? CL_MIN : op == OP_MAX ? CL_MAX : CL_ANY;
+        int j = p.d.n_cls[cl]++;
+        p.d.cls_acc[cl][j] = (unsigned char)a;
+        p.d.cls_col[cl][j] = (unsigned char)p.d.acc_col[a];
+        p.d.cls_kind[cl][j] = (unsigned char)kind;
+    }
     p.d.has_count = need_count ? 1 : 0;
     p.d.count_word = need_count ? 1 : -1;
     p.d.acc_word0 = 1 + (need_count ? 1 : 0);

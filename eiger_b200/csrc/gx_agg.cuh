@@ -40,7 +40,14 @@ struct agg_desc {
     int count_word = -1;
     int acc_word0 = 1;
     int rec_words = 2;
+    // The same accumulators grouped by update class, so hot loops run one
+    // branch-free body per class: integer SUM, float SUM, MIN, MAX, ANY.
+    int n_cls[5] = {};
+    unsigned char cls_acc[5][MAX_ACCS] = {};
+    unsigned char cls_col[5][MAX_ACCS] = {};
+    unsigned char cls_kind[5][MAX_ACCS] = {};
 };
+enum acc_class : int { CL_ISUM = 0, CL_FSUM = 1, CL_MIN = 2, CL_MAX = 3, CL_ANY = 4 };
 
 // Host-side plan: agg_desc + how to emit the reference's output columns.
 struct out_spec {
@@ -103,10 +110,11 @@ __device__ __forceinline__ uint64_t load_lane(const void* base, int width, int k
 }
 
 // v[c] for a runtime c without dynamic register indexing.
-__device__ __forceinline__ uint64_t pick(const uint64_t (&v)[MAX_VCOLS], int c) {
+template <int N>
+__device__ __forceinline__ uint64_t pick(const uint64_t (&v)[N], int c) {
     uint64_t x = v[0];
 #pragma unroll
-    for (int k = 1; k < MAX_VCOLS; ++k)
+    for (int k = 1; k < N; ++k)
         if (c == k) x = v[k];
     return x;
 }
@@ -153,6 +161,58 @@ __device__ __forceinline__ void acc_atomic(uint64_t* p, int op, int kind, uint64
     }
 }
 
+// Shared-memory update tuned for B200, where only 32-bit integer shared
+// atomics are native (64-bit ones are compare-and-swap loops, 5-30x slower):
+//   * integer SUM: two 32-bit adds — the low word's carry (detected from
+//     the returned old value) goes into the high word, so the 64-bit result
+//     is exact and wraps like the reference's u64 atomicAdd;
+//   * MIN / MAX: a plain read first; the 64-bit atomic runs only when the
+//     value would change the extreme (rare after the first rows of a group);
+//   * float SUM: the native double atomicAdd;  ANY: a plain store.
+__device__ __forceinline__ void acc_shared(uint64_t* p, int op, int kind, uint64_t v) {
+    switch (op) {
+        case OP_SUM:
+            if (kind == VK_F) {
+                atomicAdd(reinterpret_cast<double*>(p), __longlong_as_double((long long)v));
+            } else {
+                unsigned* w = reinterpret_cast<unsigned*>(p);
+                unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+                unsigned old = atomicAdd(w, lo);
+                hi += (old + lo) < old ? 1u : 0u;
+                if (hi) atomicAdd(w + 1, hi);
+            }
+            break;
+        case OP_MIN: {
+            uint64_t cur = *reinterpret_cast<volatile uint64_t*>(p);
+            bool better;
+            if (kind == VK_I) better = (long long)v < (long long)cur;
+            else if (kind == VK_U) better = v < cur;
+            else better = __longlong_as_double((long long)v) < __longlong_as_double((long long)cur);
+            if (better) acc_atomic(p, op, kind, v);
+            break;
+        }
+        case OP_MAX: {
+            uint64_t cur = *reinterpret_cast<volatile uint64_t*>(p);
+            bool better;
+            if (kind == VK_I) better = (long long)v > (long long)cur;
+            else if (kind == VK_U) better = v > cur;
+            else better = __longlong_as_double((long long)v) > __longlong_as_double((long long)cur);
+            if (better) acc_atomic(p, op, kind, v);
+            break;
+        }
+        default:
+            *reinterpret_cast<volatile unsigned long long*>(p) = v;
+            break;
+    }
+}
+
+// Identity word of an accumulator.
+__device__ __forceinline__ uint64_t acc_ident(int op, int kind) {
+    if (op == OP_MIN) return kind == VK_I ? 0x7FFFFFFFFFFFFFFFull : (kind == VK_U ? ~0ull : 0x7FF0000000000000ull);
+    if (op == OP_MAX) return kind == VK_I ? 0x8000000000000000ull : (kind == VK_U ? 0ull : 0xFFF0000000000000ull);
+    return 0ull;
+}
+
 // Non-atomic combine of two lane values (register-level reductions).
 __device__ __forceinline__ uint64_t acc_combine(int op, int kind, uint64_t a, uint64_t b) {
     switch (op) {
@@ -182,6 +242,35 @@ __device__ __forceinline__ uint64_t acc_combine(int op, int kind, uint64_t a, ui
         default:
             return b;
     }
+}
+
+// One row's update of a shared-memory table: accumulator a of `slot` lives
+// at acc[a * stride + slot].  Loops per update class (see agg_desc), each
+// with a fixed body; see acc_shared for the per-class atomics used.
+template <int NV>
+__device__ __forceinline__ void shared_row_update(uint64_t* acc, size_t stride, int slot, const agg_desc& d,
+                                                  const uint64_t (&v)[NV]) {
+    for (int j = 0; j < d.n_cls[CL_ISUM]; ++j) {
+        uint64_t x = pick(v, d.cls_col[CL_ISUM][j]);
+        unsigned* w = reinterpret_cast<unsigned*>(acc + d.cls_acc[CL_ISUM][j] * stride + slot);
+        unsigned lo = (unsigned)x, hi = (unsigned)(x >> 32);
+        unsigned old = atomicAdd(w, lo);
+        hi += (old + lo) < old ? 1u : 0u;
+        if (hi) atomicAdd(w + 1, hi);
+    }
+    for (int j = 0; j < d.n_cls[CL_FSUM]; ++j) {
+        double x = __longlong_as_double((long long)pick(v, d.cls_col[CL_FSUM][j]));
+        atomicAdd(reinterpret_cast<double*>(acc + d.cls_acc[CL_FSUM][j] * stride + slot), x);
+    }
+    for (int j = 0; j < d.n_cls[CL_MIN]; ++j)
+        acc_shared(acc + d.cls_acc[CL_MIN][j] * stride + slot, OP_MIN, d.cls_kind[CL_MIN][j],
+                   pick(v, d.cls_col[CL_MIN][j]));
+    for (int j = 0; j < d.n_cls[CL_MAX]; ++j)
+        acc_shared(acc + d.cls_acc[CL_MAX][j] * stride + slot, OP_MAX, d.cls_kind[CL_MAX][j],
+                   pick(v, d.cls_col[CL_MAX][j]));
+    for (int j = 0; j < d.n_cls[CL_ANY]; ++j)
+        *reinterpret_cast<volatile unsigned long long*>(acc + d.cls_acc[CL_ANY][j] * stride + slot) =
+            pick(v, d.cls_col[CL_ANY][j]);
 }
 
 }  // namespace dev_

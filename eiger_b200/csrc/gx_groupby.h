@@ -7,7 +7,7 @@ namespace gx {
 
 // ----- hash group-by (gx_groupby_hash.cu) -----
 void init_records(uint64_t* recs, int64_t nrec, const agg_desc& d, uint64_t empty, cudaStream_t s);
-int hash_smem_slots(const agg_desc& d, int key_width, int64_t groups_bound);
+int hash_smem_slots(const agg_desc& d, int key_width, int64_t groups_bound, int* replicas);
 void hash_groupby(const col& key, const agg_plan& p, gx_groupby_hint* hint, cudaStream_t s,
                   gx_table* out);
 

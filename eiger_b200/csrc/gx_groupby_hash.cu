@@ -18,6 +18,7 @@
 
 #include "gx_agg.cuh"
 #include "gx_groupby.h"
+#include "gx_groupby_hash_spec.cuh"
 
 namespace gx {
 namespace {
@@ -65,14 +66,19 @@ __device__ __forceinline__ uint64_t* g_find_or_insert(const gtable& t, const agg
     return nullptr;
 }
 
-__device__ __forceinline__ void g_update(uint64_t* r, const agg_desc& d, const uint64_t (&v)[MAX_VCOLS],
+template <int NV>
+__device__ __forceinline__ void g_update(uint64_t* r, const agg_desc& d, const uint64_t (&v)[NV],
                                          unsigned long long cnt) {
     if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), cnt);
     for (int a = 0; a < d.n_acc; ++a)
         dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], dev_::pick(v, d.acc_col[a]));
 }
 
-// Shared-memory table view.  Layout: keys[S] | counts[S] (u32) | acc[A][S] (u64).
+// Shared-memory table of one CTA:
+//   keys[S] (u32 or u64) | counts[R][S] (u32) | acc[R][A][S] (u64)
+// The key table is shared by the CTA; the accumulators are replicated R
+// times (warp w updates replica w % R) so that low-cardinality inputs do not
+// serialise on a handful of shared-memory words.
 template <int KW>
 struct stable {
     using kt = typename std::conditional<KW == 4, uint32_t, unsigned long long>::type;
@@ -82,6 +88,8 @@ struct stable {
     int* fill;
     uint32_t mask;
     int limit;
+    uint32_t S;
+    int R;
 };
 
 template <int KW>
@@ -108,54 +116,68 @@ __device__ __forceinline__ int s_find_or_insert(const stable<KW>& t, uint64_t kw
     return -1;
 }
 
-constexpr int HGB_NT = 512;
+constexpr int HGB_NT = 1024;
 constexpr int HGB_UNROLL = 4;
 
-template <int KW, bool SMEM>
-__global__ void __launch_bounds__(HGB_NT) k_hash_groupby(const void* __restrict__ keys, int64_t n,
-                                                          int key_kind, agg_desc d, gtable g,
-                                                          uint32_t s_slots) {
+template <int KW, bool SMEM, int NV, class... ACCS>
+__global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restrict__ keys, int64_t n,
+                                                             int key_kind, agg_desc d, gtable g,
+                                                             uint32_t s_slots, int reps) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_fill;
     stable<KW> st;
     using kt = typename stable<KW>::kt;
+    const int warp = threadIdx.x >> 5;
+    unsigned* my_counts = nullptr;
+    uint64_t* my_acc = nullptr;
     if (SMEM) {
+        const size_t S = s_slots;
+        const size_t key_bytes = (S * KW + 15) & ~size_t(15);
         st.keys = reinterpret_cast<kt*>(smem);
-        st.counts = reinterpret_cast<unsigned*>(smem + (size_t)s_slots * KW);
-        st.acc = reinterpret_cast<uint64_t*>(smem + (size_t)s_slots * (KW + 4));
+        st.counts = reinterpret_cast<unsigned*>(smem + key_bytes);
+        st.acc = reinterpret_cast<uint64_t*>(smem + key_bytes + ((S * 4 * reps + 15) & ~size_t(15)));
         st.fill = &s_fill;
         st.mask = s_slots - 1;
         st.limit = (int)(s_slots / 2);
+        st.S = s_slots;
+        st.R = reps;
         const kt EMPTY = KW == 4 ? (kt)S_EMPTY4 : (kt)S_EMPTY8;
-        for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) {
-            st.keys[i] = EMPTY;
-            st.counts[i] = 0;
-        }
-        for (int a = 0; a < d.n_acc; ++a) {
-            uint64_t idv;
-            int op = d.acc_op[a], kind = d.acc_kind[a];
-            if (op == OP_MIN) idv = kind == VK_I ? 0x7FFFFFFFFFFFFFFFull : (kind == VK_U ? ~0ull : 0x7FF0000000000000ull);
-            else if (op == OP_MAX) idv = kind == VK_I ? 0x8000000000000000ull : (kind == VK_U ? 0ull : 0xFFF0000000000000ull);
-            else idv = 0;
-            for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) st.acc[(size_t)a * s_slots + i] = idv;
-        }
+        for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) st.keys[i] = EMPTY;
+        for (uint32_t i = threadIdx.x; i < s_slots * reps; i += HGB_NT) st.counts[i] = 0;
+        for (int r = 0; r < reps; ++r)
+            for (int a = 0; a < d.n_acc; ++a) {
+                uint64_t idv = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
+                uint64_t* base = st.acc + ((size_t)r * d.n_acc + a) * S;
+                for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) base[i] = idv;
+            }
         if (threadIdx.x == 0) s_fill = 0;
+        // Spread a warp's lanes over the replicas: lanes of one warp that hit
+        // the same group then update different words.
+        const int rep = (int)(threadIdx.x % (unsigned)reps);
+        my_counts = st.counts + (size_t)rep * S;
+        my_acc = st.acc + (size_t)rep * d.n_acc * S;
         __syncthreads();
     }
 
     const int64_t tile = (int64_t)HGB_NT * HGB_UNROLL;
     for (int64_t base = blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
         uint64_t kw[HGB_UNROLL];
-        uint64_t v[HGB_UNROLL][MAX_VCOLS];
+        uint64_t v[HGB_UNROLL][NV];
 #pragma unroll
         for (int u = 0; u < HGB_UNROLL; ++u) {
             int64_t i = base + u * HGB_NT + threadIdx.x;
             if (i < n) {
                 if (KW == 4) kw[u] = canon32(__ldg(static_cast<const unsigned*>(keys) + i), key_kind);
                 else kw[u] = canon64(__ldg(static_cast<const unsigned long long*>(keys) + i), key_kind);
+                if constexpr (sizeof...(ACCS) > 0) {
 #pragma unroll
-                for (int c = 0; c < MAX_VCOLS; ++c)
-                    if (c < d.n_cols) v[u][c] = dev_::load_lane(d.col_ptr[c], d.col_width[c], d.col_kind[c], i);
+                    for (int c = 0; c < NV; ++c)
+                        v[u][c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < NV; ++c)
+                        if (c < d.n_cols) v[u][c] = dev_::load_lane(d.col_ptr[c], d.col_width[c], d.col_kind[c], i);
+                }
             }
         }
 #pragma unroll
@@ -166,10 +188,11 @@ __global__ void __launch_bounds__(HGB_NT) k_hash_groupby(const void* __restrict_
             int slot = -1;
             if (SMEM) slot = s_find_or_insert<KW>(st, kw[u], h);
             if (slot >= 0) {
-                if (d.has_count) atomicAdd(&st.counts[slot], 1u);
-                for (int a = 0; a < d.n_acc; ++a)
-                    dev_::acc_atomic(st.acc + (size_t)a * s_slots + slot, d.acc_op[a], d.acc_kind[a],
-                                     dev_::pick(v[u], d.acc_col[a]));
+                // The per-replica count is kept even without COUNT: it tells
+                // the merge which replicas saw the group (for ANY).
+                atomicAdd(&my_counts[slot], 1u);
+                if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, slot, v[u]);
+                else dev_::shared_row_update<NV>(my_acc, s_slots, slot, d, v[u]);
             } else {
                 uint64_t* r = g_find_or_insert<KW>(g, d, kw[u], h);
                 if (r) g_update(r, d, v[u], 1ull);
@@ -186,10 +209,23 @@ __global__ void __launch_bounds__(HGB_NT) k_hash_groupby(const void* __restrict_
             uint64_t kw = (uint64_t)k;
             uint64_t* r = g_find_or_insert<KW>(g, d, kw, key_hash<KW>(kw));
             if (!r) continue;
-            if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), (unsigned long long)st.counts[i]);
-            for (int a = 0; a < d.n_acc; ++a)
-                dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a],
-                                 st.acc[(size_t)a * s_slots + i]);
+            unsigned long long c = 0;
+            int first = -1;
+            for (int rp = 0; rp < reps; ++rp) {
+                unsigned cr = st.counts[(size_t)rp * s_slots + i];
+                c += cr;
+                if (cr && first < 0) first = rp;
+            }
+            if (first < 0) continue;
+            if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), c);
+            for (int a = 0; a < d.n_acc; ++a) {
+                uint64_t x = st.acc[((size_t)first * d.n_acc + a) * s_slots + i];
+                for (int rp = first + 1; rp < reps; ++rp)
+                    if (st.counts[(size_t)rp * s_slots + i])
+                        x = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], x,
+                                              st.acc[((size_t)rp * d.n_acc + a) * s_slots + i]);
+                dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], x);
+            }
         }
     }
 }
@@ -221,23 +257,90 @@ void init_records(uint64_t* recs, int64_t nrec, const agg_desc& d, uint64_t empt
     GX_LAUNCHED();
 }
 
-int hash_smem_slots(const agg_desc& d, int key_width, int64_t groups_bound) {
-    size_t per_slot = (size_t)key_width + 4 + 8 * (size_t)d.n_acc;
-    size_t budget = 100 * 1024;  // two 512-thread CTAs per SM
+// Shared-table geometry: S slots (load <= 1/2) and R accumulator replicas
+// within a 200 KB budget (one 1024-thread CTA per SM).
+int hash_smem_slots(const agg_desc& d, int key_width, int64_t groups_bound, int* replicas) {
+    const size_t budget = 200 * 1024;
+    const size_t per_rep = 4 + 8 * (size_t)d.n_acc;  // per slot per replica
     uint32_t s = 1u << 16;
-    while (s > 64 && s * per_slot > budget) s >>= 1;
+    while (s > 64 && s * (key_width + per_rep) > budget) s >>= 1;
     if (groups_bound > 0 && groups_bound < (int64_t)s / 2) {
         uint32_t want = (uint32_t)next_pow2((uint64_t)groups_bound * 2);
-        if (want < 256) want = 256;
+        if (want < 64) want = 64;
         if (want < s) s = want;
     }
+    size_t r = (budget - (size_t)s * key_width) / ((size_t)s * per_rep);
+    if (r < 1) r = 1;
+    if (r > 32) r = 32;
+    *replicas = (int)r;
     return (int)s;
+}
+
+template <int KW, bool SMEM, int NV>
+static void launch_hash_nv(int grid, size_t smem, cudaStream_t s, const void* keys, int64_t n, int kind,
+                           const agg_desc& d, const gtable& g, uint32_t slots, int reps) {
+    if (SMEM)
+        GX_CUDA(cudaFuncSetAttribute(k_hash_groupby<KW, SMEM, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    k_hash_groupby<KW, SMEM, NV><<<grid, HGB_NT, smem, s>>>(keys, n, kind, d, g, SMEM ? slots : 0, SMEM ? reps : 1);
+}
+
+// Specialised instantiations: (op, kind, column) lists over 8-byte value columns.
+template <class... ACCS>
+static bool plan_matches(const agg_desc& d) {
+    constexpr int ops[] = {ACCS::op...}, kinds[] = {ACCS::kind...}, cols[] = {ACCS::col...};
+    if (d.n_acc != (int)sizeof...(ACCS)) return false;
+    for (int c = 0; c < d.n_cols; ++c)
+        if (d.col_width[c] != 8) return false;
+    for (int a = 0; a < d.n_acc; ++a)
+        if (d.acc_op[a] != ops[a] || d.acc_kind[a] != kinds[a] || d.acc_col[a] != cols[a]) return false;
+    return true;
+}
+
+template <int KW, int NV, class... ACCS>
+static bool try_spec(int grid, size_t smem, cudaStream_t s, const void* keys, int64_t n, int kind, const agg_desc& d,
+                     const gtable& g, uint32_t slots, int reps) {
+    if (d.n_cols != NV || !plan_matches<ACCS...>(d)) return false;
+    GX_CUDA(cudaFuncSetAttribute(k_hash_groupby<KW, true, NV, ACCS...>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    k_hash_groupby<KW, true, NV, ACCS...><<<grid, HGB_NT, smem, s>>>(keys, n, kind, d, g, slots, reps);
+    return true;
+}
+
+template <int KW>
+static bool launch_spec(int grid, size_t smem, cudaStream_t s, const void* keys, int64_t n, int kind,
+                        const agg_desc& d, const gtable& g, uint32_t slots, int reps) {
+    using namespace spec;
+    // SUM(int) [+ COUNT]
+    if (try_spec<KW, 1, A<OP_SUM, VK_I, 0>>(grid, smem, s, keys, n, kind, d, g, slots, reps)) return true;
+    // SUM(double)
+    if (try_spec<KW, 1, A<OP_SUM, VK_F, 0>>(grid, smem, s, keys, n, kind, d, g, slots, reps)) return true;
+    // SUM / MIN / MAX over an int64 and a float64 column [+ COUNT]
+    if (try_spec<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_MIN, VK_I, 0>, A<OP_MAX, VK_I, 0>, A<OP_SUM, VK_F, 1>,
+                 A<OP_MIN, VK_F, 1>, A<OP_MAX, VK_F, 1>>(grid, smem, s, keys, n, kind, d, g, slots, reps))
+        return true;
+    // SUM over two int64 columns
+    if (try_spec<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_SUM, VK_I, 1>>(grid, smem, s, keys, n, kind, d, g, slots, reps))
+        return true;
+    return false;
+}
+
+template <int KW>
+static void launch_hash(bool smem_mode, int nv, int grid, size_t smem, cudaStream_t s, const void* keys, int64_t n,
+                        int kind, const agg_desc& d, const gtable& g, uint32_t slots, int reps) {
+    if (smem_mode && !getenv("GX_HASH_GENERIC") && launch_spec<KW>(grid, smem, s, keys, n, kind, d, g, slots, reps))
+        return;
+#define GX_HL(SM, NV) \
+    if (smem_mode == SM && nv == NV) return launch_hash_nv<KW, SM, NV>(grid, smem, s, keys, n, kind, d, g, slots, reps);
+    GX_HL(true, 1) GX_HL(true, 2) GX_HL(true, 4) GX_HL(true, 8)
+    GX_HL(false, 1) GX_HL(false, 2) GX_HL(false, 4) GX_HL(false, 8)
+#undef GX_HL
 }
 
 // Runs the hash group-by into a global table of `cap` records.
 // Returns false when the table overflowed (caller retries larger).
-static bool hash_groupby_run(const col& key, const agg_plan& p, uint64_t cap, int smem_mode,
-                             uint32_t s_slots, int64_t out_capacity, cudaStream_t s, gx_table* out) {
+static bool hash_groupby_run(const col& key, int out_key_type, const agg_plan& p, uint64_t cap, int smem_mode,
+                             uint32_t s_slots, int reps, int64_t out_capacity, cudaStream_t s, gx_table* out) {
     const agg_desc& d = p.d;
     int kw = size_of(key.type);
     uint64_t empty = kw == 4 ? G_EMPTY4 : G_EMPTY8;
@@ -252,25 +355,15 @@ static bool hash_groupby_run(const col& key, const agg_plan& p, uint64_t cap, in
     g.overflow = flags.get<int>() + 1;
     int kind = vkind_of(key.type);
     if (key.n > 0) {
-        size_t smem = smem_mode ? (size_t)s_slots * (kw + 4 + 8 * d.n_acc) : 0;
-        int per_sm = smem_mode ? std::max(1, std::min(2, (int)((200 * 1024) / std::max<size_t>(smem, 1)))) : 4;
-        int grid = grid_for(key.n, HGB_NT * HGB_UNROLL, per_sm);
+        size_t smem = 0;
+        if (smem_mode)
+            smem = (((size_t)s_slots * kw + 15) & ~size_t(15)) + (((size_t)s_slots * 4 * reps + 15) & ~size_t(15)) +
+                   (size_t)s_slots * reps * 8 * d.n_acc;
+        int grid = grid_for(key.n, HGB_NT * HGB_UNROLL, smem_mode ? 1 : 2);
         GX_PROF("hash_groupby", s);
-        if (kw == 4) {
-            if (smem_mode) {
-                GX_CUDA(cudaFuncSetAttribute(k_hash_groupby<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                k_hash_groupby<4, true><<<grid, HGB_NT, smem, s>>>(key.data, key.n, kind, d, g, s_slots);
-            } else {
-                k_hash_groupby<4, false><<<grid, HGB_NT, 0, s>>>(key.data, key.n, kind, d, g, 0);
-            }
-        } else {
-            if (smem_mode) {
-                GX_CUDA(cudaFuncSetAttribute(k_hash_groupby<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                k_hash_groupby<8, true><<<grid, HGB_NT, smem, s>>>(key.data, key.n, kind, d, g, s_slots);
-            } else {
-                k_hash_groupby<8, false><<<grid, HGB_NT, 0, s>>>(key.data, key.n, kind, d, g, 0);
-            }
-        }
+        int nv = d.n_cols <= 1 ? 1 : d.n_cols <= 2 ? 2 : d.n_cols <= 4 ? 4 : 8;
+        if (kw == 4) launch_hash<4>(smem_mode, nv, grid, smem, s, key.data, key.n, kind, d, g, s_slots, reps);
+        else launch_hash<8>(smem_mode, nv, grid, smem, s, key.data, key.n, kind, d, g, s_slots, reps);
         GX_LAUNCHED();
     }
     int hflags[2];
@@ -278,7 +371,7 @@ static bool hash_groupby_run(const col& key, const agg_plan& p, uint64_t cap, in
     GX_CUDA(cudaStreamSynchronize(s));
     if (hflags[1]) return false;
     emit_groupby_output(p, recs.get<uint64_t>(), (int64_t)cap + 1, true, empty, (int64_t)cap,
-                        flags.get<int>(), key.type, out_capacity, s, out);
+                        flags.get<int>(), out_key_type, out_capacity, s, out);
     return true;
 }
 
@@ -302,14 +395,15 @@ void hash_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hint, c
     int lf = hint->load_factor_pct > 0 ? hint->load_factor_pct : 50;
     lf = std::max(10, std::min(90, lf));
     uint64_t cap = next_pow2((uint64_t)std::max<int64_t>(64, bound * 100 / lf + 1));
-    uint32_t s_slots = (uint32_t)hash_smem_slots(p.d, size_of(key.type), bound_known ? bound : -1);
+    int reps = 1;
+    uint32_t s_slots = (uint32_t)hash_smem_slots(p.d, size_of(key.type), bound_known ? bound : -1, &reps);
     // Shared tables only pay off when they can hold a useful share of the
     // keys (low cardinality, or skew that concentrates rows on few keys).
     bool smem_mode = bound <= (int64_t)s_slots * 8;
     if (const char* e = getenv("GX_HASH_SMEM")) smem_mode = atoi(e) != 0;
     int64_t out_cap = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
     for (int attempt = 0; attempt < 6; ++attempt) {
-        if (hash_groupby_run(key, p, cap, smem_mode, s_slots, out_cap, s, out)) return;
+        if (hash_groupby_run(key, key_in.type, p, cap, smem_mode, s_slots, reps, out_cap, s, out)) return;
         cap *= 4;
     }
     fail(GX_EOVERFLOW, "hash group-by table overflow after retries");

@@ -1,0 +1,53 @@
+// gx_groupby_hash_spec.cuh — compile-time specialised hash group-by bodies.
+//
+// The generic kernel reads its aggregation list at run time; for the common
+// shapes (8-byte value columns, a few fixed accumulator lists) these
+// instantiations unroll the per-row update into straight-line code.  They
+// use exactly the shared-table layout, accumulator order and merge of the
+// generic kernel, so the host picks one whenever the plan matches and falls
+// back to the generic kernel otherwise.
+#pragma once
+
+namespace gx {
+namespace spec {
+
+template <int OP, int KIND, int COL>
+struct A {
+    static constexpr int op = OP, kind = KIND, col = COL;
+};
+
+template <int OP, int KIND>
+__device__ __forceinline__ void upd(uint64_t* p, uint64_t v) {
+    if constexpr (OP == OP_SUM && KIND != VK_F) {
+        unsigned* w = reinterpret_cast<unsigned*>(p);
+        unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+        unsigned old = atomicAdd(w, lo);
+        hi += (old + lo) < old ? 1u : 0u;
+        if (hi) atomicAdd(w + 1, hi);
+    } else if constexpr (OP == OP_SUM) {
+        atomicAdd(reinterpret_cast<double*>(p), __longlong_as_double((long long)v));
+    } else if constexpr (OP == OP_MIN || OP == OP_MAX) {
+        uint64_t cur = *reinterpret_cast<volatile uint64_t*>(p);
+        bool better;
+        if constexpr (KIND == VK_I)
+            better = OP == OP_MIN ? (long long)v < (long long)cur : (long long)v > (long long)cur;
+        else if constexpr (KIND == VK_U)
+            better = OP == OP_MIN ? v < cur : v > cur;
+        else {
+            double x = __longlong_as_double((long long)v), c = __longlong_as_double((long long)cur);
+            better = OP == OP_MIN ? x < c : x > c;
+        }
+        if (better) dev_::acc_atomic(p, OP, KIND, v);
+    } else {
+        *reinterpret_cast<volatile unsigned long long*>(p) = v;
+    }
+}
+
+template <int I, class First, class... Rest>
+__device__ __forceinline__ void apply_all(uint64_t* acc, uint32_t S, int slot, const uint64_t* v) {
+    upd<First::op, First::kind>(acc + (size_t)I * S + slot, v[First::col]);
+    if constexpr (sizeof...(Rest) > 0) apply_all<I + 1, Rest...>(acc, S, slot, v);
+}
+
+}  // namespace spec
+}  // namespace gx

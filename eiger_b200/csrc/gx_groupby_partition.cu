@@ -282,8 +282,7 @@ __global__ void __launch_bounds__(PA_NT) k_part_agg(const void* __restrict__ pke
             }
             if (found >= 0) {
                 if (d.has_count) atomicAdd(&scnt[found], 1u);
-                for (int a = 0; a < d.n_acc; ++a)
-                    dev_::acc_atomic(sacc + (size_t)a * S + found, d.acc_op[a], d.acc_kind[a], dev_::pick(v, d.acc_col[a]));
+                dev_::shared_row_update<MAX_VCOLS>(sacc, S, found, d, v);
             } else {
                 if (!s_spilled) s_spilled = 1;
                 uint64_t* r = pg_find<KW>(g, d, kw, h);
@@ -455,7 +454,10 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     partition_starts(mc.out[0], kw, n, kind, R, pstart.get<int64_t>(), s);
 
     // Work units.
-    int64_t T = std::max<int64_t>(1 << 14, ceil_div(n, (int64_t)dev().sm_count * 8));
+    // Split threshold: partitions above twice the mean size are split (Zipf
+    // hot partitions), and with few partitions every partition is split so
+    // that about four units per SM exist.
+    int64_t T = std::max<int64_t>(1 << 14, std::min<int64_t>(2 * ceil_div(n, P), ceil_div(n, (int64_t)dev().sm_count * 4)));
     dbuf ucount((size_t)P * 8, s), uoff((size_t)(P + 1) * 8, s);
     k_unit_counts<<<(unsigned)ceil_div(P, 256), 256, 0, s>>>(pstart.get<int64_t>(), P, T, ucount.get<int64_t>());
     GX_LAUNCHED();
@@ -467,7 +469,12 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     GX_LAUNCHED();
 
     uint64_t empty = kw == 4 ? PG_EMPTY4 : PG_EMPTY8;
+    // Split units merge through the spill table, so size it for every group
+    // when any partition was split; otherwise it only catches overflow.
+    int64_t total_units = read_scalar(uoff.get<int64_t>() + P, s);
+    int64_t live_parts = std::min<int64_t>(P, n);
     uint64_t gcap = 1u << 16;
+    if (total_units > live_parts) gcap = std::max<uint64_t>(gcap, next_pow2((uint64_t)bound * 2));
     int64_t out_cap = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
     // Output records: sized from the group bound, grown (up to n) on overflow.
     int64_t rec_cap = std::max<int64_t>(1, std::min<int64_t>(n, std::max<int64_t>(bound + bound / 4, 4096)));

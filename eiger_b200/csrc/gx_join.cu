@@ -54,23 +54,56 @@ struct build_run {
     int kind;
 };
 
-// First build position with image >= img, and the end of its equal run.
-template <int KW>
-__device__ __forceinline__ void find_run(const build_run& b, uint64_t img, int64_t* first, int64_t* last) {
-    *first = 0;
-    *last = 0;
-    if (img < b.lo || img > b.hi) return;
-    uint64_t bk = (img - b.lo) >> b.shift;
-    int64_t lo = b.dir[bk], hi = b.dir[bk + 1];
-    while (lo < hi) {
-        int64_t mid = (lo + hi) >> 1;
-        if (img_of<KW>(b.keys, mid, b.kind) < img) lo = mid + 1;
-        else hi = mid;
+// Matches of IPT probe rows against the sorted build run, with the loads of
+// all rows issued together (directory, then up to four keys of each small
+// bucket) so their L2 latencies overlap.  Equal keys share a bucket, so a
+// row's matches are the equal keys inside its bucket.
+template <int KW, int IPT>
+__device__ __forceinline__ void lookup_batch(const build_run& b, const uint64_t (&img)[IPT],
+                                             const bool (&valid)[IPT], int64_t (&first)[IPT], int (&cnt)[IPT]) {
+    uint32_t d0[IPT], d1[IPT];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        d0[k] = d1[k] = 0;
+        if (valid[k] && img[k] >= b.lo && img[k] <= b.hi) {
+            uint64_t bk = (img[k] - b.lo) >> b.shift;
+            d0[k] = __ldg(b.dir + bk);
+            d1[k] = __ldg(b.dir + bk + 1);
+        }
     }
-    int64_t e = lo;
-    while (e < b.n && img_of<KW>(b.keys, e, b.kind) == img) ++e;
-    *first = lo;
-    *last = e;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        first[k] = d0[k];
+        cnt[k] = 0;
+        uint32_t len = d1[k] - d0[k];
+        if (len <= 4) {
+            uint64_t kv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) kv[j] = (uint32_t)j < len ? img_of<KW>(b.keys, (int64_t)d0[k] + j, b.kind) : ~img[k];
+            int f = 4, c = 0;
+#pragma unroll
+            for (int j = 3; j >= 0; --j)
+                if (kv[j] == img[k]) { f = j; ++c; }
+            first[k] = (int64_t)d0[k] + f;
+            cnt[k] = c;
+        } else {
+            // lower and upper bound inside the bucket
+            int64_t lo = d0[k], hi = d1[k];
+            while (lo < hi) {
+                int64_t mid = (lo + hi) >> 1;
+                if (img_of<KW>(b.keys, mid, b.kind) < img[k]) lo = mid + 1;
+                else hi = mid;
+            }
+            int64_t lo2 = lo, hi2 = d1[k];
+            while (lo2 < hi2) {
+                int64_t mid = (lo2 + hi2) >> 1;
+                if (img_of<KW>(b.keys, mid, b.kind) <= img[k]) lo2 = mid + 1;
+                else hi2 = mid;
+            }
+            first[k] = lo;
+            cnt[k] = (int)(lo2 - lo);
+        }
+    }
 }
 
 struct probe_side {
@@ -80,22 +113,35 @@ struct probe_side {
     int kind;
 };
 
+// Tile layout shared by the count and write kernels: warp w of the block owns
+// the contiguous rows [tile + w*32*IPT, +32*IPT); row (k, lane) = k*32 + lane.
 template <int KW>
-__global__ void __launch_bounds__(JP_NT) k_probe_count(build_run b, probe_side p, int64_t* __restrict__ tile_out) {
-    int64_t base = blockIdx.x * (int64_t)JP_TILE;
-    int64_t c = 0;
+__device__ __forceinline__ void load_probe(const probe_side& p, int64_t row0, uint64_t (&img)[JP_IPT],
+                                           bool (&valid)[JP_IPT]) {
 #pragma unroll
     for (int k = 0; k < JP_IPT; ++k) {
-        int64_t i = base + k * JP_NT + threadIdx.x;
-        if (i < p.n) {
-            int64_t f, l;
-            find_run<KW>(b, img_of<KW>(p.keys, i, p.kind), &f, &l);
-            c += l - f;
-        }
+        int64_t i = row0 + k * 32;
+        valid[k] = i < p.n;
+        img[k] = valid[k] ? img_of<KW>(p.keys, i, p.kind) : 0;
     }
+}
+
+template <int KW>
+__global__ void __launch_bounds__(JP_NT) k_probe_count(build_run b, probe_side p, int64_t* __restrict__ tile_out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int64_t row0 = blockIdx.x * (int64_t)JP_TILE + warp * 32 * JP_IPT + lane;
+    uint64_t img[JP_IPT];
+    bool valid[JP_IPT];
+    int64_t first[JP_IPT];
+    int cnt[JP_IPT];
+    load_probe<KW>(p, row0, img, valid);
+    lookup_batch<KW, JP_IPT>(b, img, valid, first, cnt);
+    int64_t c = 0;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) c += cnt[k];
     __shared__ int64_t sm[JP_NT / 32];
     c = dev_::warp_sum(c);
-    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = c;
+    if (lane == 0) sm[warp] = c;
     __syncthreads();
     if (threadIdx.x == 0) {
         int64_t t = 0;
@@ -139,32 +185,40 @@ template <int KW>
 __global__ void __launch_bounds__(JP_NT) k_probe_write(build_run b, probe_side p, const int64_t* __restrict__ tile_off,
                                                         join_out o) {
     __shared__ int64_t sm[JP_NT / 32 + 1];
-    // Blocked arrangement: thread t owns rows base + t*IPT .. +IPT so the
-    // output order equals the probe order.
-    int64_t base = blockIdx.x * (int64_t)JP_TILE + threadIdx.x * (int64_t)JP_IPT;
-    int64_t f[JP_IPT], l[JP_IPT];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int64_t row0 = blockIdx.x * (int64_t)JP_TILE + warp * 32 * JP_IPT + lane;
+    uint64_t img[JP_IPT];
+    bool valid[JP_IPT];
+    int64_t first[JP_IPT];
+    int cnt[JP_IPT];
+    load_probe<KW>(p, row0, img, valid);
+    lookup_batch<KW, JP_IPT>(b, img, valid, first, cnt);
     int64_t mine = 0;
 #pragma unroll
-    for (int k = 0; k < JP_IPT; ++k) {
-        int64_t i = base + k;
-        f[k] = l[k] = 0;
-        if (i < p.n) find_run<KW>(b, img_of<KW>(p.keys, i, p.kind), &f[k], &l[k]);
-        mine += l[k] - f[k];
-    }
+    for (int k = 0; k < JP_IPT; ++k) mine += cnt[k];
+    int64_t wtot = dev_::warp_sum(mine);
+    // Exclusive prefix over the warps of the tile (warp-major = row order).
     int64_t total;
-    int64_t pos = tile_off[blockIdx.x] + dev_::block_exclusive_sum<JP_NT, int64_t>(mine, sm, &total);
+    int64_t wbase = dev_::block_exclusive_sum<JP_NT, int64_t>(lane == 0 ? wtot : 0, sm, &total);
+    wbase = __shfl_sync(0xffffffffu, wbase, 0) + tile_off[blockIdx.x];
+    int64_t running = 0;
+#pragma unroll
     for (int k = 0; k < JP_IPT; ++k) {
-        int64_t i = base + k;
-        for (int64_t m = f[k]; m < l[k]; ++m, ++pos) {
+        int64_t inc = dev_::warp_inclusive_sum((int64_t)cnt[k]);
+        int64_t pos = wbase + running + inc - cnt[k];
+        running += __shfl_sync(0xffffffffu, inc, 31);
+        int64_t i = row0 + k * 32;
+        for (int m = 0; m < cnt[k]; ++m, ++pos) {
+            int64_t bm = first[k] + m;
             int64_t prow = p.rowid ? p.rowid[i] : i;
-            if (o.key) st_w(o.key, o.key_width, pos, ld_w(b.keys, o.key_width, m));
+            if (o.key) st_w(o.key, o.key_width, pos, ld_w(b.keys, o.key_width, bm));
             for (int c = 0; c < o.n_pay; ++c) {
                 uint64_t v;
                 switch (o.src[c]) {
-                    case 0: v = ld_w(b.vals, b.val_width, m); break;
-                    case 1: v = ld_w(o.col[c], o.width[c], (int64_t)ld_w(b.vals, 8, m)); break;
+                    case 0: v = ld_w(b.vals, b.val_width, bm); break;
+                    case 1: v = ld_w(o.col[c], o.width[c], (int64_t)ld_w(b.vals, 8, bm)); break;
                     case 2: v = ld_w(o.col[c], o.width[c], prow); break;
-                    case 3: v = ld_w(b.vals, 8, m); break;
+                    case 3: v = ld_w(b.vals, 8, bm); break;
                     default: v = (uint64_t)prow; break;
                 }
                 st_w(o.out[c], o.width[c], pos, v);
@@ -191,10 +245,189 @@ struct sorted_side {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Dense unique build keys.  When the build keys are unique and span at most
+// four times their count, ordering them is a counting sort whose rank is the
+// key itself: row i lands at position image(key_i) - min.  The placed row ids
+// (uint32, 4 B per position: 64 MB for 2^24 keys) stay L2-resident, and a
+// probe row finds its match with one L2 read instead of a search.
+// ---------------------------------------------------------------------------
+constexpr uint32_t NO_ROW = 0xFFFFFFFFu;
+
+template <int KW>
+__global__ void k_dense_place(const void* __restrict__ keys, int64_t n, int kind, uint64_t lo,
+                              uint32_t* __restrict__ slot_row, int* __restrict__ dup) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t pos = img_of<KW>(keys, i, kind) - lo;
+        uint32_t old = atomicCAS(slot_row + pos, NO_ROW, (uint32_t)i);
+        if (old != NO_ROW) atomicExch(dup, 1);
+    }
+}
+
+template <int KW>
+__device__ __forceinline__ void dense_lookup(const void* pkeys, int64_t np, int kind, uint64_t lo, uint64_t hi,
+                                             const uint32_t* slot_row, int64_t row0, uint32_t (&m)[JP_IPT]) {
+    uint64_t img[JP_IPT];
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) {
+        int64_t i = row0 + k * 32;
+        img[k] = i < np ? img_of<KW>(pkeys, i, kind) : hi + 1;
+    }
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k)
+        m[k] = (img[k] >= lo && img[k] <= hi) ? __ldg(slot_row + (img[k] - lo)) : NO_ROW;
+}
+
+template <int KW>
+__global__ void __launch_bounds__(JP_NT) k_dense_count(const void* __restrict__ pkeys, int64_t np, int kind,
+                                                        uint64_t lo, uint64_t hi,
+                                                        const uint32_t* __restrict__ slot_row,
+                                                        int64_t* __restrict__ tile_out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int64_t row0 = blockIdx.x * (int64_t)JP_TILE + warp * 32 * JP_IPT + lane;
+    uint32_t m[JP_IPT];
+    dense_lookup<KW>(pkeys, np, kind, lo, hi, slot_row, row0, m);
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) c += m[k] != NO_ROW;
+    __shared__ int sm[JP_NT / 32];
+    c = dev_::warp_sum(c);
+    if (lane == 0) sm[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t t = 0;
+        for (int j = 0; j < JP_NT / 32; ++j) t += sm[j];
+        tile_out[blockIdx.x] = t;
+    }
+}
+
+// Output sources for the dense path: 1 = build column at the build row,
+// 2 = probe column at the probe row, 3 = build row id, 4 = probe row id.
+template <int KW>
+__global__ void __launch_bounds__(JP_NT) k_dense_write(const void* __restrict__ pkeys, int64_t np, int kind,
+                                                        uint64_t lo, uint64_t hi,
+                                                        const uint32_t* __restrict__ slot_row,
+                                                        const int64_t* __restrict__ tile_off, join_out o) {
+    __shared__ int64_t sm[JP_NT / 32 + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int64_t row0 = blockIdx.x * (int64_t)JP_TILE + warp * 32 * JP_IPT + lane;
+    uint32_t m[JP_IPT];
+    dense_lookup<KW>(pkeys, np, kind, lo, hi, slot_row, row0, m);
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) c += m[k] != NO_ROW;
+    int64_t wtot = dev_::warp_sum((int64_t)c);
+    int64_t total;
+    int64_t wbase = dev_::block_exclusive_sum<JP_NT, int64_t>(lane == 0 ? wtot : 0, sm, &total);
+    wbase = __shfl_sync(0xffffffffu, wbase, 0) + tile_off[blockIdx.x];
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) {
+        bool hit = m[k] != NO_ROW;
+        unsigned bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            int64_t pos = wbase + __popc(bal & lt);
+            int64_t i = row0 + k * 32;
+            if (o.key) st_w(o.key, o.key_width, pos, ld_w(pkeys, o.key_width, i));
+            for (int cc = 0; cc < o.n_pay; ++cc) {
+                uint64_t v;
+                switch (o.src[cc]) {
+                    case 1: v = ld_w(o.col[cc], o.width[cc], (int64_t)m[k]); break;
+                    case 2: v = ld_w(o.col[cc], o.width[cc], i); break;
+                    case 3: v = (uint64_t)m[k]; break;
+                    default: v = (uint64_t)i; break;
+                }
+                st_w(o.out[cc], o.width[cc], pos, v);
+            }
+        }
+        wbase += __popc(bal);
+    }
+}
+
 struct join_inputs {
     col lkey, rkey;
     std::vector<col> lpay, rpay;
 };
+
+// Output columns of a join: [key, left payloads.., right payloads..] or the
+// row-id pair; `dense` selects the source codes of the dense path.
+static join_out make_outputs(const join_inputs& in, bool build_left, bool rowids_only, bool pay_in_run, bool dense,
+                             int64_t total, cudaStream_t s, gx_table* out) {
+    join_out o;
+    std::memset(&o, 0, sizeof(o));
+    out->cols.clear();
+    const int kw = size_of(in.lkey.type);
+    if (rowids_only) {
+        out->cols.push_back(make_col(GX_INT64, total, s));
+        out->cols.push_back(make_col(GX_INT64, total, s));
+        o.n_pay = 2;
+        o.out[0] = out->cols[0].buf.get(); o.width[0] = 8; o.src[0] = build_left ? 3 : 4;
+        o.out[1] = out->cols[1].buf.get(); o.width[1] = 8; o.src[1] = build_left ? 4 : 3;
+        return o;
+    }
+    out->cols.push_back(make_col(in.lkey.type, total, s));
+    o.key = out->cols[0].buf.get();
+    o.key_width = kw;
+    auto add_side = [&](bool is_build, const std::vector<col>& pays) {
+        for (size_t c = 0; c < pays.size(); ++c) {
+            int w = size_of(pays[c].type);
+            require(w > 0, "join: STRING payload columns are not supported");
+            out->cols.push_back(make_col(pays[c].type, total, s));
+            int j = o.n_pay++;
+            o.out[j] = out->cols.back().buf.get();
+            o.width[j] = w;
+            o.col[j] = pays[c].data;
+            o.src[j] = is_build ? (dense ? 1 : (pay_in_run ? 0 : 1)) : 2;
+        }
+    };
+    if (build_left) { add_side(true, in.lpay); add_side(false, in.rpay); }
+    else { add_side(false, in.lpay); add_side(true, in.rpay); }
+    return o;
+}
+
+// Returns false when the build keys turn out not to be unique.
+static bool dense_join(const join_inputs& in, const gx_join_hint& hint, bool rowids_only, bool build_left,
+                       uint64_t lo, uint64_t hi, cudaStream_t s, gx_table* out) {
+    const col& bkey = build_left ? in.lkey : in.rkey;
+    const col& pkey = build_left ? in.rkey : in.lkey;
+    const int kw = size_of(in.lkey.type);
+    const int kind = vkind_of(in.lkey.type);
+    const int64_t nb = bkey.n, np = pkey.n;
+    uint64_t npos = hi - lo + 1;
+    dbuf slot_row((size_t)npos * 4, s), flag(8, s);
+    fill_u32(slot_row.get(), NO_ROW, (int64_t)npos, s);
+    GX_CUDA(cudaMemsetAsync(flag.get(), 0, 8, s));
+    {
+        GX_PROF("join_build_place", s);
+        if (kw == 4) k_dense_place<4><<<grid_for(nb, 256, 8), 256, 0, s>>>(bkey.data, nb, kind, lo, slot_row.get<uint32_t>(), flag.get<int>());
+        else k_dense_place<8><<<grid_for(nb, 256, 8), 256, 0, s>>>(bkey.data, nb, kind, lo, slot_row.get<uint32_t>(), flag.get<int>());
+        GX_LAUNCHED();
+    }
+    if (read_scalar(flag.get<int>(), s)) return false;
+    int64_t ntiles = ceil_div(std::max<int64_t>(np, 1), JP_TILE);
+    dbuf tc(ntiles * 8, s), toff((ntiles + 1) * 8, s);
+    int64_t total = 0;
+    if (np > 0) {
+        GX_PROF("join_probe_count", s);
+        if (kw == 4) k_dense_count<4><<<(unsigned)ntiles, JP_NT, 0, s>>>(pkey.data, np, kind, lo, hi, slot_row.get<uint32_t>(), tc.get<int64_t>());
+        else k_dense_count<8><<<(unsigned)ntiles, JP_NT, 0, s>>>(pkey.data, np, kind, lo, hi, slot_row.get<uint32_t>(), tc.get<int64_t>());
+        GX_LAUNCHED();
+        exclusive_scan_i64(tc.get<int64_t>(), toff.get<int64_t>(), ntiles, s);
+        total = read_scalar(toff.get<int64_t>() + ntiles, s);
+    }
+    if (hint.max_out > 0 && total > hint.max_out)
+        fail(GX_EOVERFLOW, "join output (" + std::to_string(total) + " rows) exceeds hint.max_out (" +
+                               std::to_string(hint.max_out) + ")");
+    join_out o = make_outputs(in, build_left, rowids_only, false, true, total, s, out);
+    if (total > 0) {
+        GX_PROF("join_probe_write", s);
+        if (kw == 4) k_dense_write<4><<<(unsigned)ntiles, JP_NT, 0, s>>>(pkey.data, np, kind, lo, hi, slot_row.get<uint32_t>(), toff.get<int64_t>(), o);
+        else k_dense_write<8><<<(unsigned)ntiles, JP_NT, 0, s>>>(pkey.data, np, kind, lo, hi, slot_row.get<uint32_t>(), toff.get<int64_t>(), o);
+        GX_LAUNCHED();
+    }
+    GX_CUDA(cudaStreamSynchronize(s));
+    return true;
+}
 
 // Core: returns owned output columns in order [key?, left payloads.., right payloads..]
 // or [left_rowid, right_rowid] when rowids_only.
@@ -213,13 +446,17 @@ static void join_core(const join_inputs& in, const gx_join_hint& hint, bool rowi
     require((int)bpay.size() <= MAX_PAY && (int)ppay.size() <= MAX_PAY, "join: too many payload columns");
 
     const int64_t nb = bkey.n, np = pkey.n;
+    uint64_t lo = 0, hi = 0;
+    if (nb > 0) key_image_range(bkey, &lo, &hi, s);
+    uint64_t span = hi - lo;
+    // Dense unique build keys: place rows by key instead of comparison sorting.
+    if (nb > 0 && hint.sort_mode == GX_JOIN_SORTED_BUILD && nb < (int64_t)NO_ROW && span < (uint64_t)nb * 4 &&
+        dense_join(in, hint, rowids_only, build_left, lo, hi, s, out))
+        return;
     // Sort the build side: (key, payload) when exactly one 4/8-byte payload.
     bool pay_in_run = !rowids_only && bpay.size() == 1 && (size_of(bpay[0].type) == 4 || size_of(bpay[0].type) == 8);
     int vw = pay_in_run ? size_of(bpay[0].type) : 8;
     dbuf bk((size_t)std::max<int64_t>(nb, 1) * kw, s), bv((size_t)std::max<int64_t>(nb, 1) * vw, s);
-    uint64_t lo = 0, hi = 0;
-    if (nb > 0) key_image_range(bkey, &lo, &hi, s);
-    uint64_t span = hi - lo;
     int nbits = span == 0 ? 1 : 64 - __builtin_clzll(span);
     if (nb > 0) {
         if (pay_in_run) radix_sort_biased(bkey, bpay[0].data, vw, false, 0, nbits, false, lo, bk.get(), bv.get(), nullptr, 0, s);
@@ -267,36 +504,7 @@ static void join_core(const join_inputs& in, const gx_join_hint& hint, bool rowi
         fail(GX_EOVERFLOW, "join output (" + std::to_string(total) + " rows) exceeds hint.max_out (" +
                                std::to_string(hint.max_out) + ")");
 
-    join_out o;
-    std::memset(&o, 0, sizeof(o));
-    out->cols.clear();
-    if (rowids_only) {
-        out->cols.push_back(make_col(GX_INT64, total, s));
-        out->cols.push_back(make_col(GX_INT64, total, s));
-        o.n_pay = 2;
-        // left row id, right row id
-        o.out[0] = out->cols[0].buf.get(); o.width[0] = 8; o.src[0] = build_left ? 3 : 4;
-        o.out[1] = out->cols[1].buf.get(); o.width[1] = 8; o.src[1] = build_left ? 4 : 3;
-    } else {
-        out->cols.push_back(make_col(in.lkey.type, total, s));
-        o.key = out->cols[0].buf.get();
-        o.key_width = kw;
-        auto add_side = [&](bool is_build, const std::vector<col>& pays) {
-            for (size_t c = 0; c < pays.size(); ++c) {
-                int w = size_of(pays[c].type);
-                require(w > 0, "join: STRING payload columns are not supported");
-                out->cols.push_back(make_col(pays[c].type, total, s));
-                int j = o.n_pay++;
-                o.out[j] = out->cols.back().buf.get();
-                o.width[j] = w;
-                o.col[j] = pays[c].data;
-                o.src[j] = is_build ? (pay_in_run ? 0 : 1) : 2;
-            }
-        };
-        // Output order is always [key, left payloads, right payloads].
-        if (build_left) { add_side(true, in.lpay); add_side(false, in.rpay); }
-        else { add_side(false, in.lpay); add_side(true, in.rpay); }
-    }
+    join_out o = make_outputs(in, build_left, rowids_only, pay_in_run, false, total, s, out);
     if (total > 0) {
         GX_PROF("join_probe_write", s);
         if (kw == 4) k_probe_write<4><<<(unsigned)ntiles, JP_NT, 0, s>>>(br, ps, toff.get<int64_t>(), o);
