@@ -307,6 +307,8 @@ def run_sweep(args) -> None:
     zs = [float(z) for z in args.sweep_zipf.split(",")]
     algos = {"hash": gx.HASH, "sort": gx.SORT, "partition": gx.PARTITION}
     reqs = groupby_reqs(gx)
+    if args.sweep_reqs == "sumcount":
+        reqs = [(0, gx.SUM), (0, gx.COUNT_ALL)]
     for kdt in args.sweep_keys.split(","):
         tdt = torch.int32 if kdt == "int32" else torch.int64
         for z in zs:
@@ -335,7 +337,8 @@ def run_sweep(args) -> None:
                         ng = r.num_rows
                         del r
                         ms = time_steps(torch, step, args.steps, 2) / args.steps
-                        alg = rows * (kb + 16) + ng * (kb + 56)
+                        vb, ob = (8, 16) if args.sweep_reqs == "sumcount" else (16, 56)
+                        alg = rows * (kb + vb) + ng * (kb + ob)
                         print(json.dumps({"key": kdt, "zipf": z, "groups": G, "algo": name, "ms": round(ms, 3),
                                           "mrows_s": round(rows / ms / 1e3, 1),
                                           "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4),
@@ -414,6 +417,7 @@ def main() -> None:
     ap.add_argument("--sweep-zipf", default="0")
     ap.add_argument("--sweep-keys", default="int32")
     ap.add_argument("--sweep-algos", default="hash,sort,partition")
+    ap.add_argument("--sweep-reqs", default="all", choices=["all", "sumcount"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -31,6 +31,15 @@ void generate_permutation(const gx_column_view& v, uint64_t seed, int64_t base_v
 void radix_sort_biased(const col& keys_c, const void* vals_in, int val_width, bool vals_iota, int begin_bit,
                        int end_bit, bool descending, uint64_t bias, void* keys_out, void* vals_out, void* temp,
                        size_t temp_bytes, cudaStream_t s);
+void selector_features(const col& key, float* f, cudaStream_t s);
+int64_t selector_param_count();
+void selector_load(const uint16_t* params, const float* mean, const float* stdv);
+void selector_predict(const float* feats, int rows, float* scores, cudaStream_t s);
+void mlp_forward(const void* params, const float* x, int rows, float* out, cudaStream_t s);
+void mlp_forward_backward(const void* params, const float* x, const float* tgt, const float* mask, int rows,
+                          float* grads, float* loss, cudaStream_t s);
+void mlp_adam(float* master, void* params, const float* grads, float* m, float* v, int step, float lr,
+              cudaStream_t s);
 }  // namespace gx
 
 namespace {
@@ -377,6 +386,42 @@ gx_status gx_compute_min_max(gx_column_view c, gx_stream_t s, void* mn, void* mx
     GX_TRY({
         gx::require(mn && mx, "null output");
         gx::compute_min_max(resolve(c), mn, mx, cs(s));
+    })
+}
+
+gx_status gx_selector_features(gx_column_view key, gx_stream_t s, float* features) {
+    GX_TRY({
+        gx::require(features != nullptr, "null output");
+        col k = resolve(key);
+        gx::require(gx::is_numeric(k.type), "selector: numeric key column required");
+        gx::selector_features(k, features, cs(s));
+    })
+}
+int64_t gx_selector_param_count(void) { return gx::selector_param_count(); }
+gx_status gx_selector_load(const uint16_t* params, const float* mean, const float* stdv) {
+    GX_TRY({
+        gx::require(params != nullptr, "null weights");
+        gx::selector_load(params, mean, stdv);
+    })
+}
+gx_status gx_selector_predict(const float* features, int32_t rows, float* scores) {
+    GX_TRY({
+        gx::require(features && scores && rows >= 0, "bad arguments");
+        gx::selector_predict(features, rows, scores, nullptr);
+    })
+}
+gx_status gx_mlp_forward(const void* params, const float* x, int32_t rows, float* out, gx_stream_t s) {
+    GX_TRY({ gx::mlp_forward(params, x, rows, out, cs(s)); })
+}
+gx_status gx_mlp_forward_backward(const void* params, const float* x, const float* target, const float* mask,
+                                  int32_t rows, float* grads, float* loss, gx_stream_t s) {
+    GX_TRY({ gx::mlp_forward_backward(params, x, target, mask, rows, grads, loss, cs(s)); })
+}
+gx_status gx_mlp_adam_step(float* master, void* params, const float* grads, float* m, float* v, int32_t step,
+                           float lr, gx_stream_t s) {
+    GX_TRY({
+        gx::require(step >= 1, "adam: step counts from 1");
+        gx::mlp_adam(master, params, grads, m, v, step, lr, cs(s));
     })
 }
 

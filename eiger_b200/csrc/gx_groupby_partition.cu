@@ -389,22 +389,26 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     const int kw = size_of(key.type);
     const int kind = vkind_of(key.type);
     const agg_desc& d = p.d;
-    // Shared table: 1 CTA per SM with ~200 KB.
+    // Shared table of one partition: small on purpose.  Random shared-memory
+    // atomics on B200 cost roughly one pass per distinct 128-byte segment a
+    // warp touches, so a partition's table is sized for its expected groups
+    // (a few hundred bytes per accumulator) rather than for the whole SM:
+    // the radix bits are chosen so each partition holds about 16 groups.
     size_t per_slot = 8 + 4 + 8 * (size_t)d.n_acc;
-    uint32_t S = 1u << 14;
-    while (S > 256 && S * per_slot > 200 * 1024) S >>= 1;
+    uint32_t S_max = 1u << 14;
+    while (S_max > 256 && S_max * per_slot > 200 * 1024) S_max >>= 1;
     int64_t bound = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
     if (!(hint->groups_upper_bound > 0 && hint->groups_upper_bound < n) && n > (1 << 16))
         bound = std::min<int64_t>(n, ndv_estimate(key, s) * 9 / 8 + 64);
+    int64_t gpp = 16;
+    if (const char* e = getenv("GX_PART_GROUPS")) gpp = std::max<int64_t>(1, atoll(e));
     int R = hint->radix_bits;
-    if (R <= 0) {
-        int64_t per_part = std::max<int64_t>(1, (int64_t)S / 2);
-        R = ilog2_ceil((uint64_t)std::max<int64_t>(1, ceil_div(bound, per_part)));
-        R = std::max(1, std::min(16, R));
-    }
+    if (R <= 0) R = ilog2_ceil((uint64_t)std::max<int64_t>(1, ceil_div(bound, gpp)));
     R = std::max(1, std::min(16, R));
     hint->radix_bits = R;
     const int P = 1 << R;
+    // Four slots per expected group absorbs the spread of groups across partitions.
+    uint32_t S = (uint32_t)std::min<uint64_t>(S_max, std::max<uint64_t>(64, next_pow2((uint64_t)ceil_div(bound, P) * 4)));
 
     // Partitioned copies.
     move_cols mc;
@@ -489,7 +493,8 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
         pglobal g{grec.get<uint64_t>(), gcap - 1, flags.get<int>(), flags.get<int>() + 1};
         if (n > 0) {
             size_t smem = (size_t)S * per_slot;
-            int grid = dev().sm_count;
+            int per_sm = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / std::max<size_t>(smem, 1)));
+            int grid = dev().sm_count * per_sm;
             move_cols pv;
             std::memset(&pv, 0, sizeof(pv));
             if (!gfur)
