@@ -156,7 +156,11 @@ def _load() -> C.CDLL:
         "gx_generate_keys": ([cv, C.POINTER(GenSpec), vp], i32),
         "gx_generate_values": ([cv, C.POINTER(GenSpec), vp], i32),
         "gx_generate_permutation": ([cv, C.c_uint64, i64, vp], i32),
+        "gx_generate_strings": ([vp, vp, i64, vp, i64, vp, vp, vp], i32),
         "gx_fill_sequence": ([cv, i64, i64, vp], i32),
+        "gx_profile_enable": ([i32], None),
+        "gx_profile_reset": ([], None),
+        "gx_profile_read": ([C.c_char_p, C.POINTER(C.c_double), C.POINTER(i64)], i32),
         "gx_selector_features": ([cv, vp, vp], i32),
         "gx_selector_param_count": ([], i64),
         "gx_selector_load": ([vp, vp, vp], i32),

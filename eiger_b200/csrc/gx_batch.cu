@@ -1,0 +1,609 @@
+// gx_batch.cu — many uneven string group-by pipelines in one launch.
+//
+// Each instance: dictionary-encode an ARROW string column (chars + int64
+// offsets, src/cuda/string/string_column.hpp:22-90), keep rows with
+// lo <= date < hi, and group the kept rows by the encoded key with SUM of an
+// int64 fixed-point amount and COUNT.  The reference runs such a pipeline as
+// separate operators per table (hash group-by on the STRING key after a
+// select, src/cuda/operators/groupby/groupby_hash.cu:437-498,
+// src/cuda/operators/select/select.hpp:15-64), with host syncs in between.
+//
+// Batched engine: one persistent kernel walks a work queue of row tiles of
+// all instances (dynamic tile handout -> no tail effect from uneven sizes).
+// A row finds or inserts its string in its instance's table — one 64-bit
+// word per slot holding a 24-bit hash tag and the representative row, so a
+// single CAS publishes a new entry and the bytes are compared against the
+// representative row of the input — gets the next dictionary code on
+// insert, and adds its amount / count to the slot when it passes the date
+// filter.  A finalize kernel writes the per-code results.  Both kernels and
+// the resets are captured once into a CUDA graph and replayed.  Tile size and
+// table load factor are chosen by timing the candidates on the batch.
+//
+// The plain engine (gx_batch_run_per_instance) runs the same work as one
+// operator sequence per instance: string dictionary encode, filter with
+// compaction, hash group-by on the codes.
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "gx_groupby.h"
+
+struct gx_batch_plan;
+
+namespace gx {
+
+void hash_groupby(const col& key, const agg_plan& p, gx_groupby_hint* hint, cudaStream_t s, gx_table* out);
+
+namespace {
+
+constexpr uint64_t ROW_MASK = (1ull << 40) - 1;
+
+struct inst_dev {
+    const char* chars;
+    const int64_t* offsets;
+    const int32_t* date;
+    const int64_t* amount;
+    int64_t rows;
+    int32_t lo, hi;
+    int64_t table_off;   // slot offset of this instance's table
+    int64_t result_off;  // code offset of this instance's results
+};
+
+struct work_item {
+    int32_t inst;
+    int32_t pad;
+    int64_t begin, end;
+};
+
+struct batch_dev {
+    const inst_dev* inst;
+    const work_item* work;
+    int64_t n_work;
+    unsigned long long* entries;  // [total slots]: tag << 40 | (row + 1); 0 = empty
+    unsigned* code_of_slot;
+    unsigned long long* sum_slot;
+    unsigned long long* cnt_slot;
+    unsigned* dict_size;          // per instance
+    unsigned long long* work_counter;
+    int* overflow;
+    uint32_t slots;               // per instance (power of two)
+    uint32_t max_distinct;
+    // finalize outputs (code order)
+    long long* out_sum;
+    long long* out_cnt;
+    long long* out_first;
+    long long* out_groups;        // per instance
+};
+
+__device__ __forceinline__ uint64_t fnv1a(const char* p, int64_t len) {
+    uint64_t h = 0xcbf29ce484222325ull;
+    for (int64_t i = 0; i < len; ++i) {
+        h ^= (uint8_t)p[i];
+        h *= 0x100000001b3ull;
+    }
+    return h;
+}
+
+__device__ __forceinline__ bool str_eq(const char* a, int64_t la, const char* b, int64_t lb) {
+    if (la != lb) return false;
+    for (int64_t i = 0; i < la; ++i)
+        if (a[i] != b[i]) return false;
+    return true;
+}
+
+// Find or insert row r's string; returns the slot (or -1 on a full table).
+__device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst_dev& in, int inst_id, int64_t r,
+                                                  bool* inserted) {
+    *inserted = false;
+    const int64_t o0 = in.offsets[r], o1 = in.offsets[r + 1];
+    const char* s = in.chars + o0;
+    const int64_t len = o1 - o0;
+    const uint64_t h = fnv1a(s, len);
+    const uint64_t tag = h >> 40;
+    const uint64_t mine = (tag << 40) | (uint64_t)(r + 1);
+    const uint32_t mask = b.slots - 1;
+    uint32_t slot = (uint32_t)h & mask;
+    unsigned long long* tab = b.entries + in.table_off;
+    for (uint32_t p = 0; p <= mask; ++p) {
+        unsigned long long e = ((volatile unsigned long long*)tab)[slot];
+        if (e == 0) {
+            unsigned long long old = atomicCAS(tab + slot, 0ull, (unsigned long long)mine);
+            if (old == 0) {
+                *inserted = true;
+                return in.table_off + slot;
+            }
+            e = old;
+        }
+        if ((e >> 40) == tag) {
+            int64_t rr = (int64_t)(e & ROW_MASK) - 1;
+            if (str_eq(in.chars + in.offsets[rr], in.offsets[rr + 1] - in.offsets[rr], s, len))
+                return in.table_off + slot;
+        }
+        slot = (slot + 1) & mask;
+    }
+    atomicExch(b.overflow, 1);
+    (void)inst_id;
+    return -1;
+}
+
+__global__ void __launch_bounds__(256) k_batch_main(batch_dev b) {
+    __shared__ long long s_item;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            unsigned long long w = atomicAdd(b.work_counter, 1ull);
+            s_item = w < (unsigned long long)b.n_work ? (long long)w : -1;
+        }
+        __syncthreads();
+        const long long w = s_item;
+        __syncthreads();
+        if (w < 0) break;
+        const work_item it = b.work[w];
+        const inst_dev in = b.inst[it.inst];
+        for (int64_t r = it.begin + threadIdx.x; r < it.end; r += blockDim.x) {
+            bool ins;
+            int64_t slot = find_or_insert(b, in, it.inst, r, &ins);
+            if (slot < 0) continue;
+            if (ins) b.code_of_slot[slot] = atomicAdd(&b.dict_size[it.inst], 1u);
+            int32_t dt = in.date[r];
+            if (dt >= in.lo && dt < in.hi) {
+                atomicAdd(&b.sum_slot[slot], (unsigned long long)in.amount[r]);
+                atomicAdd(&b.cnt_slot[slot], 1ull);
+            }
+        }
+    }
+}
+
+// Per-code results from the slot tables (grid over all slots).
+__global__ void k_batch_finalize(batch_dev b, int n_inst) {
+    const int64_t total = (int64_t)n_inst * b.slots;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
+        unsigned long long e = b.entries[g];
+        if (e == 0) continue;
+        const int inst = (int)(g / b.slots);
+        const unsigned code = b.code_of_slot[g];
+        if (code >= b.max_distinct) {
+            atomicExch(b.overflow, 1);
+            continue;
+        }
+        const int64_t o = b.inst[inst].result_off + code;
+        const unsigned long long c = b.cnt_slot[g];
+        b.out_sum[o] = (long long)b.sum_slot[g];
+        b.out_cnt[o] = (long long)c;
+        b.out_first[o] = (long long)(e & ROW_MASK) - 1;
+        if (c) atomicAdd((unsigned long long*)&b.out_groups[inst], 1ull);
+    }
+}
+
+// ---- plain-engine pieces -------------------------------------------------
+struct enc_dev {
+    const char* chars;
+    const int64_t* offsets;
+    int64_t rows;
+    unsigned long long* entries;
+    unsigned* code_of_slot;
+    unsigned* dict_size;
+    int* overflow;
+    uint32_t slots;
+    int32_t* codes;
+};
+
+__device__ __forceinline__ int64_t enc_find(const enc_dev& e, int64_t r, bool insert, bool* inserted) {
+    batch_dev b;
+    b.entries = e.entries;
+    b.slots = e.slots;
+    b.overflow = e.overflow;
+    inst_dev in;
+    in.chars = e.chars;
+    in.offsets = e.offsets;
+    in.table_off = 0;
+    if (insert) return find_or_insert(b, in, 0, r, inserted);
+    // lookup only: the insert pass has published every string
+    *inserted = false;
+    const int64_t o0 = e.offsets[r], len = e.offsets[r + 1] - o0;
+    const uint64_t h = fnv1a(e.chars + o0, len), tag = h >> 40;
+    const uint32_t mask = e.slots - 1;
+    uint32_t slot = (uint32_t)h & mask;
+    for (uint32_t p = 0; p <= mask; ++p) {
+        unsigned long long en = e.entries[slot];
+        if (en == 0) return -1;
+        if ((en >> 40) == tag) {
+            int64_t rr = (int64_t)(en & ROW_MASK) - 1;
+            if (str_eq(e.chars + e.offsets[rr], e.offsets[rr + 1] - e.offsets[rr], e.chars + o0, len)) return slot;
+        }
+        slot = (slot + 1) & mask;
+    }
+    return -1;
+}
+
+__global__ void k_enc_insert(enc_dev e) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < e.rows; r += (int64_t)gridDim.x * blockDim.x) {
+        bool ins;
+        int64_t s = enc_find(e, r, true, &ins);
+        if (s >= 0 && ins) e.code_of_slot[s] = atomicAdd(e.dict_size, 1u);
+    }
+}
+__global__ void k_enc_lookup(enc_dev e) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < e.rows; r += (int64_t)gridDim.x * blockDim.x) {
+        bool ins;
+        int64_t s = enc_find(e, r, false, &ins);
+        e.codes[r] = s >= 0 ? (int32_t)e.code_of_slot[s] : -1;
+    }
+}
+
+// Filter with compaction: rows with lo <= date < hi keep (code, amount).
+constexpr int FT = 256, FIPT = 8;
+__global__ void __launch_bounds__(FT) k_filter_count(const int32_t* __restrict__ date, int64_t n, int32_t lo, int32_t hi,
+                                                     int64_t* __restrict__ tile_cnt) {
+    int64_t base = blockIdx.x * (int64_t)FT * FIPT;
+    int c = 0;
+    for (int k = 0; k < FIPT; ++k) {
+        int64_t i = base + k * FT + threadIdx.x;
+        if (i < n) c += date[i] >= lo && date[i] < hi;
+    }
+    __shared__ int sm[FT / 32];
+    int w = dev_::warp_sum(c);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = w;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int j = 0; j < FT / 32; ++j) t += sm[j];
+        tile_cnt[blockIdx.x] = t;
+    }
+}
+__global__ void __launch_bounds__(FT) k_filter_write(const int32_t* __restrict__ date, const int32_t* __restrict__ codes,
+                                                     const int64_t* __restrict__ amount, int64_t n, int32_t lo,
+                                                     int32_t hi, const int64_t* __restrict__ tile_off,
+                                                     int32_t* __restrict__ out_codes, int64_t* __restrict__ out_amt) {
+    __shared__ int64_t sm[FT / 32 + 1];
+    int64_t base = blockIdx.x * (int64_t)FT * FIPT;
+    int64_t run = tile_off[blockIdx.x];
+    for (int k = 0; k < FIPT; ++k) {
+        int64_t i = base + k * FT + threadIdx.x;
+        int keep = (i < n && date[i] >= lo && date[i] < hi) ? 1 : 0;
+        int64_t total;
+        int64_t pos = run + dev_::block_exclusive_sum<FT, int64_t>(keep, sm, &total);
+        if (keep) {
+            out_codes[pos] = codes[i];
+            out_amt[pos] = amount[i];
+        }
+        run += total;
+    }
+}
+
+__global__ void k_scatter_codes(const int32_t* __restrict__ gcode, const int64_t* __restrict__ gsum,
+                                const int64_t* __restrict__ gcnt, int64_t groups, long long* __restrict__ out_sum,
+                                long long* __restrict__ out_cnt) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < groups; g += (int64_t)gridDim.x * blockDim.x) {
+        out_sum[gcode[g]] = gsum[g];
+        out_cnt[gcode[g]] = gcnt[g];
+    }
+}
+__global__ void k_first_rows(const unsigned long long* __restrict__ entries, const unsigned* __restrict__ code_of_slot,
+                             uint32_t slots, long long* __restrict__ out_first) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < slots; s += (int64_t)gridDim.x * blockDim.x) {
+        unsigned long long e = entries[s];
+        if (e) out_first[code_of_slot[s]] = (long long)(e & ROW_MASK) - 1;
+    }
+}
+
+}  // namespace
+}  // namespace gx
+
+struct gx_batch_plan {
+    std::vector<gx_batch_instance> inst;
+    std::vector<gx::inst_dev> hinst;
+    int64_t max_distinct = 0;
+    uint32_t slots = 0;
+    int tile_rows = 4096;
+    int lf_pct = 50;
+    gx::dbuf d_inst, d_work, entries, code_of_slot, sum_slot, cnt_slot, dict_size, ctrl;
+    gx::dbuf out_sum, out_cnt, out_first, out_groups;
+    int64_t n_work = 0;
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    bool last_plain = false;
+};
+
+namespace gx {
+
+static void batch_layout(gx_batch_plan* p, int tile, int lf, cudaStream_t s) {
+    const int n = (int)p->inst.size();
+    p->tile_rows = tile;
+    p->lf_pct = lf;
+    p->slots = (uint32_t)next_pow2((uint64_t)std::max<int64_t>(64, p->max_distinct * 100 / lf + 1));
+    std::vector<work_item> work;
+    p->hinst.resize(n);
+    for (int i = 0; i < n; ++i) {
+        const gx_batch_instance& b = p->inst[i];
+        inst_dev d;
+        d.chars = b.chars;
+        d.offsets = b.offsets;
+        d.date = b.date;
+        d.amount = b.amount;
+        d.rows = b.rows;
+        d.lo = b.date_lo;
+        d.hi = b.date_hi;
+        d.table_off = (int64_t)i * p->slots;
+        d.result_off = (int64_t)i * p->max_distinct;
+        p->hinst[i] = d;
+        for (int64_t r = 0; r < b.rows; r += tile) work.push_back({i, 0, r, std::min<int64_t>(b.rows, r + tile)});
+    }
+    p->n_work = (int64_t)work.size();
+    p->d_inst = dbuf(sizeof(inst_dev) * std::max(n, 1), s);
+    p->d_work = dbuf(sizeof(work_item) * std::max<int64_t>(p->n_work, 1), s);
+    GX_CUDA(cudaMemcpyAsync(p->d_inst.get(), p->hinst.data(), sizeof(inst_dev) * n, cudaMemcpyHostToDevice, s));
+    if (p->n_work)
+        GX_CUDA(cudaMemcpyAsync(p->d_work.get(), work.data(), sizeof(work_item) * p->n_work, cudaMemcpyHostToDevice, s));
+    const size_t total_slots = (size_t)n * p->slots;
+    p->entries = dbuf(total_slots * 8, s);
+    p->code_of_slot = dbuf(total_slots * 4, s);
+    p->sum_slot = dbuf(total_slots * 8, s);
+    p->cnt_slot = dbuf(total_slots * 8, s);
+    p->dict_size = dbuf((size_t)std::max(n, 1) * 4, s);
+    p->ctrl = dbuf(16, s);
+    const size_t total_codes = (size_t)n * p->max_distinct;
+    p->out_sum = dbuf(std::max<size_t>(total_codes, 1) * 8, s);
+    p->out_cnt = dbuf(std::max<size_t>(total_codes, 1) * 8, s);
+    p->out_first = dbuf(std::max<size_t>(total_codes, 1) * 8, s);
+    p->out_groups = dbuf((size_t)std::max(n, 1) * 8, s);
+    GX_CUDA(cudaStreamSynchronize(s));
+    if (p->graph) {
+        cudaGraphExecDestroy(p->graph);
+        p->graph = nullptr;
+    }
+}
+
+static batch_dev batch_view(gx_batch_plan* p) {
+    batch_dev b;
+    b.inst = p->d_inst.get<inst_dev>();
+    b.work = p->d_work.get<work_item>();
+    b.n_work = p->n_work;
+    b.entries = p->entries.get<unsigned long long>();
+    b.code_of_slot = p->code_of_slot.get<unsigned>();
+    b.sum_slot = p->sum_slot.get<unsigned long long>();
+    b.cnt_slot = p->cnt_slot.get<unsigned long long>();
+    b.dict_size = p->dict_size.get<unsigned>();
+    b.work_counter = p->ctrl.get<unsigned long long>();
+    b.overflow = reinterpret_cast<int*>(p->ctrl.get<char>() + 8);
+    b.slots = p->slots;
+    b.max_distinct = (uint32_t)p->max_distinct;
+    b.out_sum = p->out_sum.get<long long>();
+    b.out_cnt = p->out_cnt.get<long long>();
+    b.out_first = p->out_first.get<long long>();
+    b.out_groups = p->out_groups.get<long long>();
+    return b;
+}
+
+// The whole batched run as stream work (resets, main, finalize).
+static void batch_enqueue(gx_batch_plan* p, cudaStream_t s, bool count_launches = true) {
+    const int n = (int)p->inst.size();
+    const size_t total_slots = (size_t)n * p->slots, total_codes = (size_t)n * p->max_distinct;
+    GX_CUDA(cudaMemsetAsync(p->entries.get(), 0, total_slots * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->sum_slot.get(), 0, total_slots * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->cnt_slot.get(), 0, total_slots * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->dict_size.get(), 0, (size_t)n * 4, s));
+    GX_CUDA(cudaMemsetAsync(p->ctrl.get(), 0, 16, s));
+    GX_CUDA(cudaMemsetAsync(p->out_sum.get(), 0, total_codes * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->out_cnt.get(), 0, total_codes * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->out_first.get(), 0xFF, total_codes * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->out_groups.get(), 0, (size_t)n * 8, s));
+    batch_dev b = batch_view(p);
+    k_batch_main<<<dev().sm_count * 8, 256, 0, s>>>(b);
+    GX_CUDA(cudaGetLastError());
+    k_batch_finalize<<<grid_for((int64_t)total_slots, 256, 8), 256, 0, s>>>(b, n);
+    GX_CUDA(cudaGetLastError());
+    if (count_launches) g_launches.fetch_add(2);
+}
+
+static float time_batch(gx_batch_plan* p, cudaStream_t s) {
+    cudaEvent_t a, b;
+    GX_CUDA(cudaEventCreate(&a));
+    GX_CUDA(cudaEventCreate(&b));
+    batch_enqueue(p, s);  // warm
+    GX_CUDA(cudaEventRecord(a, s));
+    batch_enqueue(p, s);
+    GX_CUDA(cudaEventRecord(b, s));
+    GX_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+}
+
+// Autotuner: time each (tile rows, load factor) candidate on this batch.
+static void batch_autotune(gx_batch_plan* p, cudaStream_t s) {
+    const int tiles[] = {1024, 4096, 16384};
+    const int lfs[] = {25, 50};
+    float best = 1e30f;
+    int bt = 4096, bl = 50;
+    if (const char* e = getenv("GX_BATCH_TILE")) {
+        batch_layout(p, atoi(e), 50, s);
+        return;
+    }
+    for (int t : tiles)
+        for (int l : lfs) {
+            batch_layout(p, t, l, s);
+            float ms = time_batch(p, s);
+            if (ms < best) { best = ms; bt = t; bl = l; }
+        }
+    batch_layout(p, bt, bl, s);
+}
+
+static void check_overflow(gx_batch_plan* p, cudaStream_t s) {
+    int ovf = read_scalar(reinterpret_cast<int*>(p->ctrl.get<char>() + 8), s);
+    if (ovf) fail(GX_EOVERFLOW, "batch: an instance exceeded max_distinct or its table filled");
+}
+
+static void batch_run(gx_batch_plan* p, cudaStream_t s) {
+    if (!p->graph || p->graph_stream != s) {
+        if (p->graph) cudaGraphExecDestroy(p->graph);
+        p->graph = nullptr;
+        cudaGraph_t g;
+        GX_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        batch_enqueue(p, s, false);
+        GX_CUDA(cudaStreamEndCapture(s, &g));
+        GX_CUDA(cudaGraphInstantiate(&p->graph, g, 0));
+        cudaGraphDestroy(g);
+        p->graph_stream = s;
+    }
+    GX_CUDA(cudaGraphLaunch(p->graph, s));
+    g_launches.fetch_add(2);
+    check_overflow(p, s);
+    p->last_plain = false;
+}
+
+// The same pipeline as one operator sequence per instance.
+static void batch_run_plain(gx_batch_plan* p, cudaStream_t s) {
+    const int n = (int)p->inst.size();
+    const size_t total_codes = (size_t)n * p->max_distinct;
+    GX_CUDA(cudaMemsetAsync(p->out_sum.get(), 0, total_codes * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->out_cnt.get(), 0, total_codes * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->out_first.get(), 0xFF, total_codes * 8, s));
+    std::vector<long long> groups(n, 0);
+    for (int i = 0; i < n; ++i) {
+        const gx_batch_instance& b = p->inst[i];
+        const int64_t rows = b.rows;
+        // 1. string dictionary encode
+        uint32_t slots = (uint32_t)next_pow2((uint64_t)std::max<int64_t>(64, p->max_distinct * 2));
+        dbuf ent((size_t)slots * 8, s), cos((size_t)slots * 4, s), ds(16, s), codes((size_t)std::max<int64_t>(rows, 1) * 4, s);
+        GX_CUDA(cudaMemsetAsync(ent.get(), 0, (size_t)slots * 8, s));
+        GX_CUDA(cudaMemsetAsync(ds.get(), 0, 16, s));
+        enc_dev e{b.chars, b.offsets, rows, ent.get<unsigned long long>(), cos.get<unsigned>(), ds.get<unsigned>(),
+                  reinterpret_cast<int*>(ds.get<char>() + 8), slots, codes.get<int32_t>()};
+        if (rows > 0) {
+            k_enc_insert<<<grid_for(rows, 256, 4), 256, 0, s>>>(e);
+            GX_LAUNCHED();
+            k_enc_lookup<<<grid_for(rows, 256, 4), 256, 0, s>>>(e);
+            GX_LAUNCHED();
+        }
+        unsigned hds[4];
+        GX_CUDA(cudaMemcpyAsync(hds, ds.get(), 16, cudaMemcpyDeviceToHost, s));
+        GX_CUDA(cudaStreamSynchronize(s));
+        if (hds[2] || hds[0] > (unsigned)p->max_distinct) fail(GX_EOVERFLOW, "batch: max_distinct exceeded");
+        // 2. filter with compaction
+        int64_t ntiles = ceil_div(std::max<int64_t>(rows, 1), FT * FIPT);
+        dbuf tc(ntiles * 8, s), toff((ntiles + 1) * 8, s);
+        k_filter_count<<<(unsigned)ntiles, FT, 0, s>>>(b.date, rows, b.date_lo, b.date_hi, tc.get<int64_t>());
+        GX_LAUNCHED();
+        exclusive_scan_i64(tc.get<int64_t>(), toff.get<int64_t>(), ntiles, s);
+        int64_t kept = read_scalar(toff.get<int64_t>() + ntiles, s);
+        dbuf kc((size_t)std::max<int64_t>(kept, 1) * 4, s), ka((size_t)std::max<int64_t>(kept, 1) * 8, s);
+        k_filter_write<<<(unsigned)ntiles, FT, 0, s>>>(b.date, codes.get<int32_t>(), b.amount, rows, b.date_lo,
+                                                      b.date_hi, toff.get<int64_t>(), kc.get<int32_t>(),
+                                                      ka.get<int64_t>());
+        GX_LAUNCHED();
+        // 3. hash group-by on the codes: SUM(amount), COUNT
+        gx_column_view vv{ka.get(), kept, GX_INT64, 0};
+        gx_table_view vt{&vv, 1};
+        gx_agg_request req[2] = {{0, GX_AGG_SUM}, {0, GX_AGG_COUNT_ALL}};
+        agg_plan plan = make_agg_plan(&vt, req, 2, false);
+        gx_groupby_hint hint;
+        gx_groupby_hint_init(&hint);
+        hint.groups_upper_bound = std::max<int64_t>(1, hds[0]);
+        hint.groupby_algo = GX_GB_HASH;
+        col kcol;
+        kcol.data = kc.get();
+        kcol.n = kept;
+        kcol.type = GX_INT32;
+        gx_table t;
+        hash_groupby(kcol, plan, &hint, s, &t);
+        const int64_t ng = t.cols[0].size;
+        const int64_t off = (int64_t)i * p->max_distinct;
+        if (ng > 0) {
+            k_scatter_codes<<<grid_for(ng, 256, 4), 256, 0, s>>>(t.cols[0].buf.get<int32_t>(), t.cols[1].buf.get<int64_t>(),
+                                                                t.cols[2].buf.get<int64_t>(), ng, p->out_sum.get<long long>() + off,
+                                                                p->out_cnt.get<long long>() + off);
+            GX_LAUNCHED();
+        }
+        k_first_rows<<<grid_for(slots, 256, 4), 256, 0, s>>>(ent.get<unsigned long long>(), cos.get<unsigned>(), slots,
+                                                           p->out_first.get<long long>() + off);
+        GX_LAUNCHED();
+        groups[i] = ng;
+        GX_CUDA(cudaStreamSynchronize(s));
+    }
+    GX_CUDA(cudaMemcpyAsync(p->out_groups.get(), groups.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    GX_CUDA(cudaStreamSynchronize(s));
+    p->last_plain = true;
+}
+
+}  // namespace gx
+
+#define GX_BTRY(...)                                       \
+    try {                                                  \
+        __VA_ARGS__;                                       \
+        return GX_OK;                                      \
+    } catch (const gx::error& e) {                         \
+        gx::set_last_error(e.what());                      \
+        return e.status;                                   \
+    } catch (const std::exception& e) {                    \
+        gx::set_last_error(e.what());                      \
+        return GX_EINVAL;                                  \
+    }
+
+namespace gx {
+void set_last_error(const char* msg);
+}
+
+extern "C" {
+
+gx_status gx_batch_plan_create(const gx_batch_instance* instances, int32_t count, int64_t max_distinct, gx_stream_t st,
+                               gx_batch_plan** plan) {
+    GX_BTRY({
+        gx::require(plan != nullptr && (count == 0 || instances != nullptr), "batch: bad arguments");
+        gx::require(count > 0, "batch: no instances");
+        gx::require(max_distinct > 0 && max_distinct < (1ll << 30), "batch: max_distinct out of range");
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(st);
+        std::unique_ptr<gx_batch_plan> p(new gx_batch_plan);
+        for (int i = 0; i < count; ++i) {
+            const gx_batch_instance& b = instances[i];
+            gx::require(b.rows >= 0 && b.rows < (1ll << 39), "batch: instance row count out of range");
+            gx::require(b.rows == 0 || (b.chars && b.offsets && b.date && b.amount), "batch: null column pointer");
+            p->inst.push_back(b);
+        }
+        p->max_distinct = max_distinct;
+        gx::batch_autotune(p.get(), s);
+        *plan = p.release();
+    })
+}
+gx_status gx_batch_run(gx_batch_plan* plan, gx_stream_t st) {
+    GX_BTRY({
+        gx::require(plan != nullptr, "batch: null plan");
+        gx::batch_run(plan, reinterpret_cast<cudaStream_t>(st));
+    })
+}
+gx_status gx_batch_run_per_instance(gx_batch_plan* plan, gx_stream_t st) {
+    GX_BTRY({
+        gx::require(plan != nullptr, "batch: null plan");
+        gx::batch_run_plain(plan, reinterpret_cast<cudaStream_t>(st));
+    })
+}
+gx_status gx_batch_results(const gx_batch_plan* plan, gx_batch_result* res) {
+    GX_BTRY({
+        gx::require(plan && res, "batch: null argument");
+        const int n = (int)plan->inst.size();
+        std::vector<long long> groups(n);
+        GX_CUDA(cudaMemcpy(groups.data(), plan->out_groups.get(), (size_t)n * 8, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; ++i) {
+            const int64_t off = (int64_t)i * plan->max_distinct;
+            res[i].num_groups = groups[i];
+            res[i].sum = plan->out_sum.get<int64_t>() + off;
+            res[i].count = plan->out_cnt.get<int64_t>() + off;
+            res[i].first_row = plan->out_first.get<int64_t>() + off;
+        }
+    })
+}
+gx_status gx_batch_tuning(const gx_batch_plan* plan, int32_t* tile_rows, int32_t* lf) {
+    GX_BTRY({
+        gx::require(plan && tile_rows && lf, "batch: null argument");
+        *tile_rows = plan->tile_rows;
+        *lf = plan->lf_pct;
+    })
+}
+void gx_batch_plan_free(gx_batch_plan* plan) {
+    if (!plan) return;
+    if (plan->graph) cudaGraphExecDestroy(plan->graph);
+    delete plan;
+}
+
+}  // extern "C"

@@ -31,6 +31,8 @@ void generate_permutation(const gx_column_view& v, uint64_t seed, int64_t base_v
 void radix_sort_biased(const col& keys_c, const void* vals_in, int val_width, bool vals_iota, int begin_bit,
                        int end_bit, bool descending, uint64_t bias, void* keys_out, void* vals_out, void* temp,
                        size_t temp_bytes, cudaStream_t s);
+void generate_strings(const char* dchars, const int64_t* doff, int64_t dsize, const int32_t* codes, int64_t rows,
+                      const int64_t* off, char* out, cudaStream_t s);
 void selector_features(const col& key, float* f, cudaStream_t s);
 int64_t selector_param_count();
 void selector_load(const uint16_t* params, const float* mean, const float* stdv);
@@ -68,6 +70,10 @@ using gx::col;
 using gx::resolve;
 
 static cudaStream_t cs(gx_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+namespace gx {
+void set_last_error(const char* msg) { t_err = msg ? msg : ""; }
+}  // namespace gx
 
 extern "C" {
 
@@ -448,6 +454,14 @@ gx_status gx_generate_values(gx_column_view out, const gx_gen_spec* sp, gx_strea
 gx_status gx_generate_permutation(gx_column_view out, uint64_t seed, int64_t base, gx_stream_t s) {
     GX_TRY({
         gx::generate_permutation(out, seed, base, cs(s));
+        GX_CUDA(cudaStreamSynchronize(cs(s)));
+    })
+}
+gx_status gx_generate_strings(const char* dict_chars, const int64_t* dict_offsets, int64_t dict_size,
+                              const int32_t* codes, int64_t rows, const int64_t* out_offsets, char* out_chars,
+                              gx_stream_t s) {
+    GX_TRY({
+        gx::generate_strings(dict_chars, dict_offsets, dict_size, codes, rows, out_offsets, out_chars, cs(s));
         GX_CUDA(cudaStreamSynchronize(cs(s)));
     })
 }

@@ -168,3 +168,28 @@ void generate_permutation(const gx_column_view& v, uint64_t seed, int64_t base_v
 }
 
 }  // namespace gx
+
+namespace gx {
+namespace {
+__global__ void k_gen_strings(const char* __restrict__ dchars, const int64_t* __restrict__ doff, int64_t dsize,
+                              const int32_t* __restrict__ codes, int64_t rows, const int64_t* __restrict__ off,
+                              char* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t c = codes[i];
+        if (c < 0 || c >= dsize) continue;
+        const int64_t s = doff[c], len = doff[c + 1] - s;
+        const int64_t o = off[i];
+        if (off[i + 1] - o != len) continue;  // offsets must match the dictionary lengths
+        for (int64_t j = 0; j < len; ++j) out[o + j] = dchars[s + j];
+    }
+}
+}  // namespace
+
+void generate_strings(const char* dchars, const int64_t* doff, int64_t dsize, const int32_t* codes, int64_t rows,
+                      const int64_t* off, char* out, cudaStream_t s) {
+    require(dchars && doff && codes && off && out, "generate_strings: null pointer");
+    if (rows <= 0) return;
+    k_gen_strings<<<grid_for(rows, 256, 8), 256, 0, s>>>(dchars, doff, dsize, codes, rows, off, out);
+    GX_LAUNCHED();
+}
+}  // namespace gx

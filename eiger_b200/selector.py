@@ -1,0 +1,250 @@
+"""Learned group-by strategy selector: data collection, training, loading.
+
+The selector scores the HASH / SORT / PARTITION group-by variants (and four
+partition fan-outs) from a sketch of a 2^14-row key sample
+(gx_selector_features).  Its network is a 3-layer FP16 MLP trained on the
+GPU with the library's own kernels (gx_mlp_forward_backward and
+gx_mlp_adam_step) on timings the plain engine produces for synthetic
+instances.  The plain NDV rule of the reference (HLL estimate <= 2^14 for
+4-byte keys / 2^18 for 8-byte keys -> HASH, else PARTITION) stays the
+fallback and the baseline for regret.
+
+    python -m eiger_b200.selector collect --instances 4096 --out timings.npz
+    python -m eiger_b200.selector train timings.npz --out eiger_b200/selector_weights.npz
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import time
+from pathlib import Path
+
+import numpy as np
+
+F, H, O = 16, 64, 7
+NV = 3               # variants: HASH, SORT, PARTITION
+FANOUTS = [8, 10, 12, 14]
+WEIGHTS = Path(__file__).resolve().parent / "selector_weights.npz"
+
+
+def _gx():
+    import eiger_b200 as gx
+    return gx
+
+
+def param_count() -> int:
+    return int(_gx().lib.gx_selector_param_count())
+
+
+# ---------------------------------------------------------------------------
+# Instances (C4: rows log-uniform in 2^16..2^28, NDV log-uniform in 1..rows,
+# Zipf s uniform in [0, 2], int32 or int64 keys; SUM + COUNT of int64 values)
+# ---------------------------------------------------------------------------
+def draw_instances(count: int, seed: int, min_log2=16, max_log2=28) -> list[dict]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        rows = int(2 ** rng.uniform(min_log2, max_log2))
+        ndv = int(max(1, round(2 ** rng.uniform(0, math.log2(rows)))))
+        out.append({"rows": rows, "ndv": ndv, "zipf": float(rng.uniform(0, 2)),
+                    "key": "int64" if rng.random() < 0.5 else "int32", "seed": int(seed * 100003 + i)})
+    return out
+
+
+def make_instance(inst: dict):
+    import torch
+    gx = _gx()
+    rows, G = inst["rows"], inst["ndv"]
+    kdt = torch.int32 if inst["key"] == "int32" else torch.int64
+    k = torch.empty(rows, dtype=kdt, device="cuda")
+    cdf = None
+    if inst["zipf"] > 0.01 and G > 1:
+        cdf = torch.from_numpy(gx.zipf_cdf(G, inst["zipf"])).cuda()
+        spec = gx.gen_spec(seed=inst["seed"], dist=gx.DIST_ZIPF, groups=G, zipf_s=inst["zipf"], scatter=1,
+                           zipf_cdf=cdf.data_ptr())
+    else:
+        spec = gx.gen_spec(seed=inst["seed"], groups=G, scatter=1)
+    gx.generate_keys(k, spec)
+    v = torch.empty(rows, dtype=torch.int64, device="cuda")
+    gx.generate_values(v, gx.gen_spec(seed=inst["seed"], stream_id=1, lo=0, hi=1 << 31))
+    return k, v, cdf
+
+
+def features(key) -> np.ndarray:
+    gx = _gx()
+    f = np.zeros(F, dtype=np.float32)
+    gx.check(gx.lib.gx_selector_features(gx.view(key), gx._stream_ptr(None), f.ctypes.data))
+    return f
+
+
+def time_call(fn, reps: int = 1) -> float:
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fn()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) / reps * 1e3
+
+
+def collect(instances: list[dict], fanout_every: int = 2, log=print) -> dict:
+    """Features and plain-engine timings (ms) of every variant per instance."""
+    import torch
+    gx = _gx()
+    reqs = [(0, gx.SUM), (0, gx.COUNT_ALL)]
+    feats, times, ftimes, heur = [], [], [], []
+    for idx, inst in enumerate(instances):
+        k, v, cdf = make_instance(inst)
+        feats.append(features(k))
+        row = []
+        for algo in (gx.HASH, gx.SORT, gx.PARTITION):
+            row.append(time_call(lambda: gx.groupby([k], [v], reqs, gx.make_hint(algo))))
+        times.append(row)
+        fr = [np.nan] * len(FANOUTS)
+        if idx % fanout_every == 0:
+            for j, bits in enumerate(FANOUTS):
+                fr[j] = time_call(lambda: gx.groupby([k], [v], reqs, gx.make_hint(gx.PARTITION, radix_bits=bits)))
+        ftimes.append(fr)
+        h = gx.make_hint(gx.AUTO_ALGO)
+        gx.groupby([k], [v], reqs, h)
+        heur.append(h.groupby_algo)
+        del k, v, cdf
+        if idx % 256 == 0:
+            torch.cuda.empty_cache()
+            log(f"collected {idx + 1}/{len(instances)}")
+    return {"features": np.array(feats, np.float32), "times": np.array(times, np.float64),
+            "fanout_times": np.array(ftimes, np.float64), "heuristic": np.array(heur, np.int32),
+            "instances": json.dumps(instances)}
+
+
+def targets_from(times: np.ndarray, ftimes: np.ndarray):
+    """log2 of the timings; unmeasured fan-outs are masked out."""
+    t = np.zeros((times.shape[0], O), np.float32)
+    m = np.zeros_like(t)
+    t[:, :NV] = np.log2(times)
+    m[:, :NV] = 1
+    ok = ~np.isnan(ftimes)
+    t[:, NV:][ok] = np.log2(ftimes[ok])
+    m[:, NV:][ok] = 1
+    return t, m
+
+
+def train(x: np.ndarray, t: np.ndarray, m: np.ndarray, epochs: int = 1500, lr: float = 3e-3, seed: int = 0):
+    """Full-batch Adam on the GPU with the library kernels; returns FP16 params."""
+    import torch
+    gx = _gx()
+    n = param_count()
+    rng = np.random.default_rng(seed)
+    w = []
+    for fan_in, fan_out in ((F, H), (H, H), (H, O)):
+        w.append(rng.normal(0, math.sqrt(2.0 / fan_in), size=(fan_out, fan_in)).reshape(-1))
+        w.append(np.zeros(fan_out))
+    master = torch.from_numpy(np.concatenate(w).astype(np.float32)).cuda()
+    assert master.numel() == n
+    params = master.half()
+    grads = torch.zeros(n, dtype=torch.float32, device="cuda")
+    mom = torch.zeros_like(grads)
+    vel = torch.zeros_like(grads)
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    dx = torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+    dt = torch.from_numpy(np.ascontiguousarray(t, np.float32)).cuda()
+    dm = torch.from_numpy(np.ascontiguousarray(m, np.float32)).cuda()
+    s = gx._stream_ptr(None)
+    hist = []
+    for step in range(1, epochs + 1):
+        gx.check(gx.lib.gx_mlp_forward_backward(params.data_ptr(), dx.data_ptr(), dt.data_ptr(), dm.data_ptr(),
+                                                x.shape[0], grads.data_ptr(), loss.data_ptr(), s))
+        gx.check(gx.lib.gx_mlp_adam_step(master.data_ptr(), params.data_ptr(), grads.data_ptr(), mom.data_ptr(),
+                                         vel.data_ptr(), step, C.c_float(lr), s))
+        if step % 100 == 0 or step == 1:
+            hist.append((step, float(loss.item())))
+    return params.cpu().numpy().view(np.uint16), hist
+
+
+def predict(params_u16: np.ndarray, x: np.ndarray) -> np.ndarray:
+    import torch
+    gx = _gx()
+    p = torch.from_numpy(params_u16.view(np.float16).copy()).cuda()
+    dx = torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+    out = torch.empty((x.shape[0], O), dtype=torch.float32, device="cuda")
+    gx.check(gx.lib.gx_mlp_forward(p.data_ptr(), dx.data_ptr(), x.shape[0], out.data_ptr(), gx._stream_ptr(None)))
+    return out.cpu().numpy()
+
+
+def regret(times: np.ndarray, choice: np.ndarray) -> float:
+    best = times.min(axis=1)
+    chosen = times[np.arange(len(choice)), choice]
+    return float(np.mean(chosen / best - 1.0))
+
+
+def heuristic_choice(heur_algo: np.ndarray) -> np.ndarray:
+    gx = _gx()
+    return np.where(heur_algo == gx.HASH, 0, np.where(heur_algo == gx.SORT, 1, 2))
+
+
+def save(path: Path, params_u16: np.ndarray, mean: np.ndarray, std: np.ndarray, meta: dict) -> None:
+    np.savez(path, params=params_u16, mean=mean.astype(np.float32), std=std.astype(np.float32),
+             meta=json.dumps(meta), version=1)
+
+
+def install(path: Path | None = None) -> bool:
+    """Load trained weights into the library (AUTO + hint.selector=LEARNED)."""
+    gx = _gx()
+    path = Path(path) if path else WEIGHTS
+    if not path.exists():
+        return False
+    d = np.load(path)
+    p = np.ascontiguousarray(d["params"], np.uint16)
+    mean = np.ascontiguousarray(d["mean"], np.float32)
+    std = np.ascontiguousarray(d["std"], np.float32)
+    gx.check(gx.lib.gx_selector_load(p.ctypes.data, mean.ctypes.data, std.ctypes.data))
+    return True
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    c = sub.add_parser("collect")
+    c.add_argument("--instances", type=int, default=4096)
+    c.add_argument("--seed", type=int, default=7)
+    c.add_argument("--out", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("timings")
+    t.add_argument("--holdout", type=int, default=1024)
+    t.add_argument("--epochs", type=int, default=3000)
+    t.add_argument("--out", default=str(WEIGHTS))
+    t.add_argument("--report", default=None)
+    a = ap.parse_args()
+    if a.cmd == "collect":
+        data = collect(draw_instances(a.instances, a.seed))
+        np.savez(a.out, **data)
+        return
+    d = np.load(a.timings)
+    x, times, ft = d["features"], d["times"], d["fanout_times"]
+    t_all, m_all = targets_from(times, ft)
+    n = x.shape[0]
+    ntr = n - a.holdout
+    mean, std = x[:ntr].mean(0), x[:ntr].std(0) + 1e-6
+    xs = (x - mean) / std
+    params, hist = train(xs[:ntr], t_all[:ntr], m_all[:ntr], epochs=a.epochs)
+    y = predict(params, xs[ntr:])
+    learned = np.argmin(y[:, :NV], axis=1)
+    heur = heuristic_choice(d["heuristic"][ntr:])
+    oracle_best = np.argmin(times[ntr:], axis=1)
+    report = {"train_instances": int(ntr), "heldout_instances": int(n - ntr),
+              "regret_learned": regret(times[ntr:], learned), "regret_heuristic": regret(times[ntr:], heur),
+              "accuracy_learned": float(np.mean(learned == oracle_best)),
+              "accuracy_heuristic": float(np.mean(heur == oracle_best)),
+              "loss_history": hist,
+              "best_variant_share": np.bincount(oracle_best, minlength=NV).tolist()}
+    save(Path(a.out), params, mean, std, report)
+    print(json.dumps(report))
+    if a.report:
+        Path(a.report).write_text(json.dumps(report, indent=1))
+
+
+if __name__ == "__main__":
+    main()

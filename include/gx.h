@@ -402,6 +402,12 @@ gx_status gx_generate_values(gx_column_view out, const gx_gen_spec* spec, gx_str
 /* Random permutation of [0, n) (n a power of two) plus `base` as int32/int64. */
 gx_status gx_generate_permutation(gx_column_view out, uint64_t seed, int64_t base,
                                   gx_stream_t stream);
+/* ARROW string column from dictionary codes: row i gets the bytes of
+ * dictionary entry codes[i] (dict_chars / dict_offsets, device); out_offsets
+ * (rows+1, device) must already hold the prefix sum of the row lengths. */
+gx_status gx_generate_strings(const char* dict_chars, const int64_t* dict_offsets, int64_t dict_size,
+                              const int32_t* codes, int64_t rows, const int64_t* out_offsets,
+                              char* out_chars, gx_stream_t stream);
 /* int64 sequence start, start+step, ... (make_sequence, column.cu:48-55). */
 gx_status gx_fill_sequence(gx_column_view out, int64_t start, int64_t step,
                            gx_stream_t stream);

@@ -87,3 +87,40 @@ def test_errors_are_reported_not_thrown():
     out = ctypes.c_void_p()
     st = gx.lib.gx_inner_eq_join(ctypes.byref(tv), ctypes.byref(tv), ctypes.byref(h), None, ctypes.byref(out))
     assert st == 1 and "auto selection" in gx.last_error()
+
+
+def test_cpp_shim_compiles_and_maps_errors_to_exceptions(tmp_path):
+    # include/gamax/gamax.hpp restates the reference's C++ operator API
+    # (namespace gamax) over the C ABI; a reference caller must compile
+    # unchanged and see std::runtime_error for a rejected call, as
+    # operators/join/join.cu:33-36 throws for a GFUR hint under AUTO.
+    src = tmp_path / "shim.cpp"
+    src.write_text('''#include <cstdio>
+#include <stdexcept>
+#include "gamax/gamax.hpp"
+using namespace gamax;
+int main() {
+  std::vector<column_view> cols{column_view(nullptr, 0, data_type{type_id::INT32}),
+                                column_view(nullptr, 0, data_type{type_id::INT32})};
+  table_view t(cols);
+  join::join_hint h;
+  h.mat_algo = join::GFUR;
+  try {
+    join::inner_eq_join(t, t, h);
+  } catch (std::runtime_error const& e) {
+    std::printf("caught:%s\\n", e.what());
+  }
+  groupby::groupby_hint gh;
+  std::printf("%d %d %lld\\n", (int)gh.groupby_algo, (int)groupby::agg_output_data_type(
+      groupby::aggregation_id::SUM, data_type{type_id::INT32}).id(), (long long)gh.groups_upper_bound);
+  return 0;
+}
+''')
+    exe = tmp_path / "shim"
+    cuda = Path("/usr/local/cuda/include")
+    subprocess.run(["g++", "-std=c++17", f"-I{ROOT / 'include'}", f"-I{cuda}", str(src), "-o", str(exe),
+                    f"-L{ROOT / 'eiger_b200'}", "-lgx", f"-Wl,-rpath,{ROOT / 'eiger_b200'}"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()
+    assert out[0].startswith("caught:") and "auto selection" in out[0]
+    algo, sum_type, bound = out[1].split()
+    assert int(algo) == 0 and int(sum_type) == int(gx.INT64) and int(bound) == 2 ** 63 - 1
