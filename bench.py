@@ -271,6 +271,37 @@ def run_gx(args) -> None:
                                      lambda m: (nb + npr) * 12 + m * 20)
         del bk, brow, pk, prow
 
+    # ----------------------------------------------------------- batched
+    batched = None
+    if args.batch_instances > 0:
+        from eiger_b200 import batch as B
+        insts, _ = B.make_instances(args.batch_instances, seed=11 + rank)
+        total = sum(it.rows for it in insts)
+        plan = B.Plan(insts, max_distinct=10_000)
+        tile, lf = plan.tuning()
+        nsteps = max(1, args.steps // 2)
+        l0 = gx.kernel_launches()
+        b_ms = time_steps(torch, plan.run, nsteps, 3, dist) / nsteps
+        b_launches = (gx.kernel_launches() - l0) // (nsteps + 3)
+        l0 = gx.kernel_launches()
+        p_ms = time_steps(torch, plan.run_per_instance, nsteps, 3, dist) / nsteps
+        p_launches = (gx.kernel_launches() - l0) // (nsteps + 3)
+        # Algorithmic bytes: every instance's strings, offsets, dates and amounts once.
+        in_b = sum(int(it.offsets[-1].item()) + (it.rows + 1) * 8 + it.rows * 12 for it in insts)
+        batched = {
+            "workload": (f"{len(insts)} string group-by pipelines, rows log-uniform in [2^12, 2^22] "
+                         f"({total} rows total): dictionary-encode ASCII keys (10^4 distinct, 8..32 bytes), "
+                         "keep 40% of rows by a date range, SUM(int64 scale-2 decimal) + COUNT per key"),
+            "rows": total, "input_bytes": in_b,
+            "batched": {"ms_per_step": b_ms, "value": world * total / (b_ms * 1e-3) / 1e6, "unit": "Mrows/s",
+                        "launches_per_step": b_launches, "hbm_frac": in_b / (b_ms * 1e-3) / 1e9 / peaks["hbm_gbs"]},
+            "per_instance": {"ms_per_step": p_ms, "value": world * total / (p_ms * 1e-3) / 1e6, "unit": "Mrows/s",
+                             "launches_per_step": p_launches},
+            "speedup": p_ms / b_ms, "tile_rows": tile, "load_factor_pct": lf,
+        }
+        del plan, insts
+        torch.cuda.empty_cache()
+
     # ------------------------------------------------------ cpu baseline
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -286,7 +317,7 @@ def run_gx(args) -> None:
                        "rows": rows, "groups": G, "groups_found": ngroups, "algo": args.algo,
                        "l2": "inputs (5.4 GB) larger than L2; no flush"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk.summary(), "join": join,
+            "clocks": clk.summary(), "join": join, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -408,6 +439,7 @@ def main() -> None:
     ap.add_argument("--algo", choices=["hash", "sort", "partition"], default="hash")
     ap.add_argument("--join-rows", type=int, default=1 << 28)
     ap.add_argument("--no-join", action="store_true")
+    ap.add_argument("--batch-instances", type=int, default=512, help="batched pipeline instances (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=1 << 24)
     ap.add_argument("--traffic", type=float, default=None,
