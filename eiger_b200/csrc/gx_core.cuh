@@ -32,6 +32,8 @@ struct error : std::runtime_error {
 inline void require(bool ok, const std::string& msg) {
     if (!ok) fail(GX_EINVAL, msg);
 }
+// Sets the calling thread's gx_last_error_message (gx_capi.cu).
+void set_last_error(const char* msg);
 
 inline void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
     if (e != cudaSuccess) {
@@ -277,6 +279,9 @@ void fill_u64(void* dst, uint64_t pattern, int64_t words, cudaStream_t s);
 void fill_u32(void* dst, uint32_t pattern, int64_t words, cudaStream_t s);
 // Exclusive scan of int64 counts into offsets (n+1 outputs, out[n] = total).
 void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
+// The same scan with its temporaries carved from caller scratch.
+size_t scan_scratch_bytes(int64_t n);
+void exclusive_scan_i64_scratch(const int64_t* in, int64_t* out, int64_t n, char* scratch, cudaStream_t s);
 // iota of int64.
 void sequence_i64(int64_t* out, int64_t n, int64_t start, int64_t step, cudaStream_t s);
 // out[i] = src[idx[i]] for `width`-byte elements.

@@ -31,6 +31,11 @@ size_t radix_temp_bytes(int64_t n, int key_width, int val_width);
 void radix_sort(const col& keys, const void* vals_in, int val_width, bool vals_iota,
                 int begin_bit, int end_bit, bool descending, void* keys_out, void* vals_out,
                 void* temp, size_t temp_bytes, cudaStream_t s);
+// Pair sort (4/8-byte keys and values) with all temporaries carved from
+// caller scratch of radix_pairs_scratch_bytes(n, kw, vw) bytes.
+size_t radix_pairs_scratch_bytes(int64_t n, int key_width, int val_width);
+void radix_sort_pairs_scratch(const col& keys, const void* vals_in, int val_width, int begin_bit, int end_bit,
+                              bool descending, void* keys_out, void* vals_out, char* scratch, cudaStream_t s);
 // Key image width in bits for a type (the default end_bit).
 inline int key_bits(int type) { return 8 * size_of(type); }
 

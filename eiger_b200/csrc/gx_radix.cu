@@ -387,3 +387,71 @@ void radix_sort(const col& keys, const void* vals_in, int val_width, bool vals_i
 }
 
 }  // namespace gx
+
+namespace gx {
+
+// Scratch bytes radix_sort_pairs_scratch needs for n pairs of 4/8-byte keys
+// and 4/8-byte values: both ping-pong halves, the per-tile digit counts and
+// offsets, and the scan's temporaries (each rounded to 256 bytes).
+size_t radix_pairs_scratch_bytes(int64_t n, int key_width, int val_width) {
+    auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
+    int64_t ntiles = ceil_div(std::max<int64_t>(n, 1), RS_TILE);
+    size_t b = r256((size_t)n * key_width) + r256((size_t)n * val_width);
+    b += r256((size_t)RS_BINS * ntiles * 8) + r256((size_t)RS_BINS * ntiles * 8 + 8);
+    return b + scan_scratch_bytes((int64_t)RS_BINS * ntiles);
+}
+
+// The pass loop of radix_sort_biased (bias 0) for 4/8-byte keys and values,
+// with every temporary taken from `scratch`.  The histogram and scatter
+// kernels are the same, so the output equals gx_sort_column_pair's.  The
+// caller has checked key/value widths and that scratch holds
+// radix_pairs_scratch_bytes(n, kw, vw).  Nothing in scratch is read before
+// it is written in the same call.
+void radix_sort_pairs_scratch(const col& keys, const void* vals_in, int val_width, int begin_bit, int end_bit,
+                              bool descending, void* keys_out, void* vals_out, char* scratch, cudaStream_t s) {
+    const int64_t n = keys.n;
+    const int kw = size_of(keys.type);
+    int full = 8 * kw;
+    if (end_bit <= 0 || end_bit > full) end_bit = full;
+    if (begin_bit < 0) begin_bit = 0;
+    if (n == 0) return;
+    auto take = [&](size_t bytes) {
+        char* p = scratch;
+        scratch += (bytes + 255) & ~size_t(255);
+        return p;
+    };
+    img_params ip{vkind_of(keys.type), kw, descending ? 1 : 0, 0};
+    int nbits = end_bit - begin_bit;
+    int passes = nbits > 0 ? (nbits + RS_MAXBITS - 1) / RS_MAXBITS : 0;
+    if (passes == 0) {
+        GX_CUDA(cudaMemcpyAsync(keys_out, keys.data, (size_t)n * kw, cudaMemcpyDeviceToDevice, s));
+        GX_CUDA(cudaMemcpyAsync(vals_out, vals_in, (size_t)n * val_width, cudaMemcpyDeviceToDevice, s));
+        return;
+    }
+    int64_t ntiles = ceil_div(n, RS_TILE);
+    char* tk = take((size_t)n * kw);
+    char* tv = take((size_t)n * val_width);
+    int64_t* counts = reinterpret_cast<int64_t*>(take((size_t)RS_BINS * ntiles * 8));
+    int64_t* offs = reinterpret_cast<int64_t*>(take((size_t)RS_BINS * ntiles * 8 + 8));
+    char* scan_tmp = scratch;
+    const void* kin = keys.data;
+    const void* vin = vals_in;
+    int shift = begin_bit;
+    for (int p = 0; p < passes; ++p) {
+        int dbits = std::min(RS_MAXBITS, end_bit - shift);
+        bool to_out = ((passes - 1 - p) % 2) == 0;
+        void* ko = to_out ? keys_out : tk;
+        void* vo = to_out ? vals_out : tv;
+        if (kw == 4) k_radix_hist<4><<<(unsigned)ntiles, RS_NT, 0, s>>>(kin, n, ip, shift, dbits, ntiles, counts);
+        else k_radix_hist<8><<<(unsigned)ntiles, RS_NT, 0, s>>>(kin, n, ip, shift, dbits, ntiles, counts);
+        GX_LAUNCHED();
+        int64_t bins = 1 << dbits;
+        exclusive_scan_i64_scratch(counts, offs, bins * ntiles, scan_tmp, s);
+        scatter_dispatch(kw, val_width, false, ntiles, s, kin, vin, n, ip, shift, dbits, offs, ko, vo);
+        kin = ko;
+        vin = vo;
+        shift += dbits;
+    }
+}
+
+}  // namespace gx

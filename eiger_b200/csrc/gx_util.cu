@@ -306,3 +306,41 @@ owned_col widen_to_32(const col& c, cudaStream_t s) {
 }
 
 }  // namespace gx
+
+namespace gx {
+
+// Scratch-carved form of exclusive_scan_i64: the per-tile sums and prefixes
+// of every level come from `scratch` (scan_scratch_bytes(n) bytes), so the
+// scan itself allocates nothing.  Same kernels, same results.
+size_t scan_scratch_bytes(int64_t n) {
+    size_t b = 0;
+    while (n > 0) {
+        int64_t t = ceil_div(n, SCAN_TILE);
+        b += (((size_t)t * 8 + 255) & ~size_t(255)) + (((size_t)(t + 1) * 8 + 255) & ~size_t(255));
+        if (t == 1) break;
+        n = t;
+    }
+    return b;
+}
+
+void exclusive_scan_i64_scratch(const int64_t* in, int64_t* out, int64_t n, char* scratch, cudaStream_t s) {
+    if (n <= 0) {
+        fill_u64(out, 0, 1, s);
+        return;
+    }
+    int64_t ntiles = ceil_div(n, SCAN_TILE);
+    int64_t* sums = reinterpret_cast<int64_t*>(scratch);
+    scratch += ((size_t)ntiles * 8 + 255) & ~size_t(255);
+    int64_t* pref = reinterpret_cast<int64_t*>(scratch);
+    scratch += ((size_t)(ntiles + 1) * 8 + 255) & ~size_t(255);
+    k_tile_sums<<<(unsigned)ntiles, SCAN_NT, 0, s>>>(in, n, sums);
+    GX_LAUNCHED();
+    if (ntiles == 1) fill_u64(pref, 0, 1, s);
+    else exclusive_scan_i64_scratch(sums, pref, ntiles, scratch, s);
+    k_tile_scan<<<(unsigned)ntiles, SCAN_NT, 0, s>>>(in, n, pref, out);
+    GX_LAUNCHED();
+    k_set_last<<<1, 32, 0, s>>>(pref, ntiles, sums, out, n);
+    GX_LAUNCHED();
+}
+
+}  // namespace gx

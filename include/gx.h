@@ -310,6 +310,23 @@ gx_status gx_sort_column(gx_column_view col, int32_t begin_bit, int32_t end_bit,
 gx_status gx_argsort(gx_column_view col, int32_t begin_bit, int32_t end_bit, int32_t order,
                      void* d_temp, size_t temp_bytes, gx_stream_t stream,
                      gx_column* key_out, gx_column* idx_out);
+/* gx_sort_column_pair without any memory allocation; no counterpart in the
+ * reference.  Same stable sort, same result, written into caller device
+ * buffers key_out / val_out (size*width bytes each, overlapping neither
+ * each other nor the inputs).  For callers that cannot allocate: an engine
+ * whose buffer manager owns all of device memory, or one that cannot take
+ * the device synchronisation an allocation may cause.  Temporaries come from
+ * one fixed 8 MiB array in device memory: keys and values 4 or 8 bytes wide,
+ * and a sort needing more scratch (about 0.5 M pairs of 8+8 bytes) fails
+ * with GX_EINVAL before any launch.  No scratch byte has to start at zero.
+ * All calls on a device share the array, so calls that overlap on the
+ * device race; order them on one stream or with events.  The first call on
+ * a device looks up the array's address (cudaGetSymbolAddress, which may
+ * load device code) and sets a kernel attribute: make it before any stream
+ * capture begins.  Returns without waiting for the sort to finish. */
+gx_status gx_sort_column_pair_noalloc(gx_column_view key, gx_column_view val, int32_t begin_bit,
+                                      int32_t end_bit, int32_t order, void* key_out,
+                                      void* val_out, gx_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
 /* Radix partition — gamax::partition                                      */
