@@ -33,7 +33,7 @@ MAT_AUTO, MAT_GFUR, MAT_GFTR, MAT_INDEX_CLUSTER = range(4)
 SORTED_BUILD, SORT_MERGE = 0, 1
 ASCENDING, DESCENDING = 0, 1
 SELECT_HEURISTIC, SELECT_LEARNED = 0, 1
-DIST_UNIFORM, DIST_CYCLIC, DIST_ZIPF, DIST_SEQUENCE = range(4)
+DIST_UNIFORM, DIST_CYCLIC, DIST_ZIPF, DIST_SEQUENCE, DIST_ZIPF_APPROX = range(5)
 
 STATUS = {0: "GX_OK", 1: "GX_EINVAL", 2: "GX_ENOMEM", 3: "GX_ECUDA", 4: "GX_EOVERFLOW",
           5: "GX_ETIMEOUT", 6: "GX_EUNSUPPORTED"}
@@ -425,6 +425,18 @@ def dictionary_encode_with_dict(col, dictionary, encode_type=INT32, stream=None)
     check(lib.gx_dictionary_encode_with_dict(view(col), view(dictionary), encode_type, _stream_ptr(stream),
                                              C.byref(o)))
     return owned_to_torch(o)
+
+
+def dictionary_encode_strings(chars, offsets, rows: int | None = None, row_offset: int = 0, size_hint: int = 0,
+                              stream=None):
+    """Hash-encode an ARROW string column (device chars + int64 offsets):
+    returns (int32 codes, NDV)."""
+    n = (offsets.numel() - 1 - row_offset) if rows is None else rows
+    sc = StringColumns(chars.data_ptr(), offsets.data_ptr())
+    v = ColumnView(C.cast(C.pointer(sc), C.c_void_p), n, STRING, row_offset)
+    o, nd = OwnedColumn(), C.c_int64()
+    check(lib.gx_dictionary_encode_strings(v, size_hint, _stream_ptr(stream), C.byref(o), C.byref(nd)))
+    return owned_to_torch(o), nd.value
 
 
 def compute_ndv_approx(col, stream=None) -> int:

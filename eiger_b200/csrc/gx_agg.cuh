@@ -161,6 +161,19 @@ __device__ __forceinline__ void acc_atomic(uint64_t* p, int op, int kind, uint64
     }
 }
 
+// Would v move the MIN / MAX accumulator `cur`?  Doubles compare in the
+// order the sign-split integer atomics of acc_atomic impose (-0.0 below
+// +0.0); NaN never improves, as NaN never participates.
+__device__ __forceinline__ bool improves(int op, int kind, uint64_t v, uint64_t cur) {
+    if (kind == VK_I) return op == OP_MIN ? (long long)v < (long long)cur : (long long)v > (long long)cur;
+    if (kind == VK_U) return op == OP_MIN ? v < cur : v > cur;
+    const double d = __longlong_as_double((long long)v);
+    if (d != d) return false;
+    const uint64_t a = v ^ (((long long)v >> 63) ? ~0ull : 0x8000000000000000ull);
+    const uint64_t b = cur ^ (((long long)cur >> 63) ? ~0ull : 0x8000000000000000ull);
+    return op == OP_MIN ? a < b : a > b;
+}
+
 // Shared-memory update tuned for B200, where only 32-bit integer shared
 // atomics are native (64-bit ones are compare-and-swap loops, 5-30x slower):
 //   * integer SUM: two 32-bit adds — the low word's carry (detected from
@@ -182,24 +195,10 @@ __device__ __forceinline__ void acc_shared(uint64_t* p, int op, int kind, uint64
                 if (hi) atomicAdd(w + 1, hi);
             }
             break;
-        case OP_MIN: {
-            uint64_t cur = *reinterpret_cast<volatile uint64_t*>(p);
-            bool better;
-            if (kind == VK_I) better = (long long)v < (long long)cur;
-            else if (kind == VK_U) better = v < cur;
-            else better = __longlong_as_double((long long)v) < __longlong_as_double((long long)cur);
-            if (better) acc_atomic(p, op, kind, v);
+        case OP_MIN:
+        case OP_MAX:
+            if (improves(op, kind, v, *reinterpret_cast<volatile uint64_t*>(p))) acc_atomic(p, op, kind, v);
             break;
-        }
-        case OP_MAX: {
-            uint64_t cur = *reinterpret_cast<volatile uint64_t*>(p);
-            bool better;
-            if (kind == VK_I) better = (long long)v > (long long)cur;
-            else if (kind == VK_U) better = v > cur;
-            else better = __longlong_as_double((long long)v) > __longlong_as_double((long long)cur);
-            if (better) acc_atomic(p, op, kind, v);
-            break;
-        }
         default:
             *reinterpret_cast<volatile unsigned long long*>(p) = v;
             break;

@@ -300,8 +300,12 @@ struct gx_batch_plan {
     gx::dbuf out_sum, out_cnt, out_first, out_groups;
     int64_t n_work = 0;
     cudaGraphExec_t graph = nullptr;
-    cudaStream_t graph_stream = nullptr;
+    cudaStream_t capture_stream = nullptr;  // private: the legacy default stream cannot be captured
     bool last_plain = false;
+    ~gx_batch_plan() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+    }
 };
 
 namespace gx {
@@ -436,16 +440,24 @@ static void check_overflow(gx_batch_plan* p, cudaStream_t s) {
 }
 
 static void batch_run(gx_batch_plan* p, cudaStream_t s) {
-    if (!p->graph || p->graph_stream != s) {
-        if (p->graph) cudaGraphExecDestroy(p->graph);
-        p->graph = nullptr;
-        cudaGraph_t g;
-        GX_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        batch_enqueue(p, s, false);
-        GX_CUDA(cudaStreamEndCapture(s, &g));
-        GX_CUDA(cudaGraphInstantiate(&p->graph, g, 0));
+    if (!p->graph) {
+        // Capture once on the plan's own stream; the executable graph is then
+        // launched on whatever stream the caller passes.
+        if (!p->capture_stream) GX_CUDA(cudaStreamCreateWithFlags(&p->capture_stream, cudaStreamNonBlocking));
+        GX_CUDA(cudaStreamSynchronize(s));  // the capture records work only; inputs are ready
+        cudaGraph_t g = nullptr;
+        GX_CUDA(cudaStreamBeginCapture(p->capture_stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            batch_enqueue(p, p->capture_stream, false);
+        } catch (...) {
+            cudaStreamEndCapture(p->capture_stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        GX_CUDA(cudaStreamEndCapture(p->capture_stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&p->graph, g, 0);
         cudaGraphDestroy(g);
-        p->graph_stream = s;
+        GX_CUDA(e);
     }
     GX_CUDA(cudaGraphLaunch(p->graph, s));
     g_launches.fetch_add(2);
@@ -527,6 +539,54 @@ static void batch_run_plain(gx_batch_plan* p, cudaStream_t s) {
     p->last_plain = true;
 }
 
+// Hash dictionary encode of one ARROW string column: int32 codes, dense in
+// [0, NDV) in first-insert order (the reference's hash encode semantics for
+// numeric keys, src/cuda/compress/dictionary_encode.cu:71-96; its
+// dictionary_encode rejects STRING, dictionary_encode.cu:32-34).  The table
+// is the plain engine's (hash tag + representative row per slot); without a
+// size hint it starts at 2^22 distinct strings and grows by 4x on overflow.
+static void dictionary_encode_strings(const gx_column_view& v, int64_t size_hint, cudaStream_t s, gx_column* out,
+                                      int64_t* ndv) {
+    require(v.type == GX_STRING, "dictionary_encode_strings: STRING column required");
+    require(v.size >= 0 && v.offset >= 0, "dictionary_encode_strings: negative size or offset");
+    const int64_t rows = v.size;
+    owned_col codes = make_col(GX_INT32, rows, s);
+    int64_t distinct = 0;
+    if (rows > 0) {
+        require(v.data != nullptr, "dictionary_encode_strings: null string columns");
+        const gx_string_columns* sc = static_cast<const gx_string_columns*>(v.data);
+        require(sc->chars && sc->offsets, "dictionary_encode_strings: null chars or offsets");
+        int64_t bound = size_hint > 0 ? std::min(size_hint, rows) : std::min<int64_t>(rows, 1 << 22);
+        bool done = false;
+        for (int attempt = 0; attempt < 8 && !done; ++attempt) {
+            uint32_t slots = (uint32_t)next_pow2((uint64_t)std::max<int64_t>(64, 2 * bound));
+            dbuf ent((size_t)slots * 8, s), cos((size_t)slots * 4, s), ds(16, s);
+            GX_CUDA(cudaMemsetAsync(ent.get(), 0, (size_t)slots * 8, s));
+            GX_CUDA(cudaMemsetAsync(ds.get(), 0, 16, s));
+            enc_dev e{sc->chars, sc->offsets + v.offset, rows, ent.get<unsigned long long>(), cos.get<unsigned>(),
+                      ds.get<unsigned>(), reinterpret_cast<int*>(ds.get<char>() + 8), slots, codes.buf.get<int32_t>()};
+            k_enc_insert<<<grid_for(rows, 256, 4), 256, 0, s>>>(e);
+            GX_LAUNCHED();
+            unsigned hds[4];
+            GX_CUDA(cudaMemcpyAsync(hds, ds.get(), 16, cudaMemcpyDeviceToHost, s));
+            GX_CUDA(cudaStreamSynchronize(s));
+            if (hds[2]) {  // table full: grow
+                require(bound < rows, "dictionary_encode_strings: table overflow");
+                bound = std::min(rows, bound * 4);
+                continue;
+            }
+            k_enc_lookup<<<grid_for(rows, 256, 4), 256, 0, s>>>(e);
+            GX_LAUNCHED();
+            GX_CUDA(cudaStreamSynchronize(s));
+            distinct = hds[0];
+            done = true;
+        }
+        require(done, "dictionary_encode_strings: table overflow after retries");
+    }
+    *ndv = distinct;
+    *out = to_gx_column(std::move(codes));
+}
+
 }  // namespace gx
 
 #define GX_BTRY(...)                                       \
@@ -601,9 +661,16 @@ gx_status gx_batch_tuning(const gx_batch_plan* plan, int32_t* tile_rows, int32_t
     })
 }
 void gx_batch_plan_free(gx_batch_plan* plan) {
-    if (!plan) return;
-    if (plan->graph) cudaGraphExecDestroy(plan->graph);
-    delete plan;
+    delete plan;  // the destructor releases the graph and the capture stream
+}
+
+gx_status gx_dictionary_encode_strings(gx_column_view col, int64_t dictionary_size_hint, gx_stream_t st,
+                                       gx_column* codes, int64_t* dict_size) {
+    GX_BTRY({
+        gx::require(codes && dict_size, "null output");
+        gx::dictionary_encode_strings(col, dictionary_size_hint, reinterpret_cast<cudaStream_t>(st), codes,
+                                      dict_size);
+    })
 }
 
 }  // extern "C"

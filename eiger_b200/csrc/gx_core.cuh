@@ -37,6 +37,9 @@ void set_last_error(const char* msg);
 
 inline void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
     if (e != cudaSuccess) {
+        // Clear the runtime's per-thread last error (for errors that do not
+        // poison the context) so a later launch check does not report it again.
+        (void)cudaGetLastError();
         fail(e == cudaErrorMemoryAllocation ? GX_ENOMEM : GX_ECUDA,
              std::string(what) + " failed: " + cudaGetErrorString(e) + " at " + file + ":" +
                  std::to_string(line));

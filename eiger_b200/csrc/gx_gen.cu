@@ -69,6 +69,19 @@ __device__ __forceinline__ uint64_t draw_rank(const gx_gen_spec& sp, uint64_t ba
             return (uint64_t)(lo < (int64_t)G ? lo : (int64_t)G - 1);
         }
         case GX_DIST_SEQUENCE: return i;
+        case GX_DIST_ZIPF_APPROX: {
+            // Invert F(x) = ((x+1)^(1-s) - 1) / ((G+1)^(1-s) - 1) (ln form at s = 1),
+            // the continuous counterpart of P(rank r) ∝ 1/(r+1)^s.
+            double u = (double)(rng_at(base, i) >> 11) * 0x1.0p-53;
+            double s = sp.zipf_s, x;
+            if (fabs(s - 1.0) < 1e-6) x = exp(u * log((double)G + 1.0)) - 1.0;
+            else {
+                double a = 1.0 - s;
+                x = pow(1.0 + u * (pow((double)G + 1.0, a) - 1.0), 1.0 / a) - 1.0;
+            }
+            uint64_t r = x > 0.0 ? (uint64_t)x : 0;
+            return r < G ? r : G - 1;
+        }
         default: return mulhi64(rng_at(base, i), G);
     }
 }

@@ -70,8 +70,17 @@ template <int NV>
 __device__ __forceinline__ void g_update(uint64_t* r, const agg_desc& d, const uint64_t (&v)[NV],
                                          unsigned long long cnt) {
     if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), cnt);
-    for (int a = 0; a < d.n_acc; ++a)
-        dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], dev_::pick(v, d.acc_col[a]));
+    for (int a = 0; a < d.n_acc; ++a) {
+        const int op = d.acc_op[a], kind = d.acc_kind[a];
+        const uint64_t x = dev_::pick(v, d.acc_col[a]);
+        uint64_t* p = r + d.acc_word0 + a;
+        if (op == OP_MIN || op == OP_MAX) {
+            // A plain (possibly stale) read first: extremes only tighten, so a
+            // stale value can only cause an unneeded atomic, never a lost one.
+            if (!dev_::improves(op, kind, x, *p)) continue;
+        }
+        dev_::acc_atomic(p, op, kind, x);
+    }
 }
 
 // Shared-memory table of one CTA:

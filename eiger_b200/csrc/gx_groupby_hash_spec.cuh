@@ -27,17 +27,7 @@ __device__ __forceinline__ void upd(uint64_t* p, uint64_t v) {
     } else if constexpr (OP == OP_SUM) {
         atomicAdd(reinterpret_cast<double*>(p), __longlong_as_double((long long)v));
     } else if constexpr (OP == OP_MIN || OP == OP_MAX) {
-        uint64_t cur = *reinterpret_cast<volatile uint64_t*>(p);
-        bool better;
-        if constexpr (KIND == VK_I)
-            better = OP == OP_MIN ? (long long)v < (long long)cur : (long long)v > (long long)cur;
-        else if constexpr (KIND == VK_U)
-            better = OP == OP_MIN ? v < cur : v > cur;
-        else {
-            double x = __longlong_as_double((long long)v), c = __longlong_as_double((long long)cur);
-            better = OP == OP_MIN ? x < c : x > c;
-        }
-        if (better) dev_::acc_atomic(p, OP, KIND, v);
+        if (dev_::improves(OP, KIND, v, *reinterpret_cast<volatile uint64_t*>(p))) dev_::acc_atomic(p, OP, KIND, v);
     } else {
         *reinterpret_cast<volatile unsigned long long*>(p) = v;
     }

@@ -344,6 +344,127 @@ __global__ void __launch_bounds__(JP_NT) k_dense_write(const void* __restrict__ 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Single-pass dense probe: count, place and write in one kernel.  With unique
+// build keys a probe row has at most one match, so the output fits in
+// `np` rows and can be allocated before the probe.  Tiles take their index
+// from an atomic ticket (so every tile a block waits on belongs to a block
+// that started earlier), publish their match count, and find their output
+// start by a decoupled look-back over the predecessors' published counts
+// (Merrill & Garland, "Single-pass Parallel Prefix Scan with Decoupled
+// Look-back", NVIDIA TR 2016).  Probe keys are read and looked up once
+// instead of twice.  Every wait is bounded: a tile that gives up sets *err,
+// publishes anyway so its successors do not wait on it, and writes nothing;
+// the host then reruns the two-pass probe.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long TS_AGG = 1ull << 62, TS_INC = 2ull << 62, TS_VAL = (1ull << 62) - 1;
+constexpr int LOOKBACK_SPIN_LIMIT = 1 << 20;
+
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Exclusive output start of `tile` (warp 0 calls it; all lanes get the value).
+__device__ __forceinline__ int64_t lookback(unsigned long long* tstate, int64_t tile, int64_t total, int* err) {
+    const int lane = threadIdx.x & 31;
+    if (tile == 0) {
+        if (lane == 0) st_release_u64(tstate, TS_INC | (unsigned long long)total);
+        return 0;
+    }
+    if (lane == 0) st_release_u64(tstate + tile, TS_AGG | (unsigned long long)total);
+    int64_t excl = 0, end = tile - 1;  // lane j looks at tile end - j
+    int spins = 0;
+    while (true) {
+        int64_t j = end - lane;
+        unsigned long long st = j >= 0 ? ld_acquire_u64(tstate + j) : TS_INC;
+        unsigned inc = __ballot_sync(0xffffffffu, (st >> 62) == 2);
+        unsigned none = __ballot_sync(0xffffffffu, (st >> 62) == 0);
+        int stop = inc ? __ffs(inc) - 1 : 31;  // nearest inclusive predecessor, else the whole window
+        unsigned need = stop == 31 ? 0xffffffffu : ((2u << stop) - 1u);
+        if (none & need) {
+            if (++spins > LOOKBACK_SPIN_LIMIT) {
+                if (lane == 0) atomicExch(err, 1);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        int64_t v = (lane <= stop && j >= 0) ? (int64_t)(st & TS_VAL) : 0;
+        excl += dev_::warp_sum(v);
+        if (inc) break;
+        end -= 32;
+    }
+    if (lane == 0) st_release_u64(tstate + tile, TS_INC | (unsigned long long)(excl + total));
+    return excl;
+}
+
+template <int KW>
+__global__ void __launch_bounds__(JP_NT) k_dense_probe1(const void* __restrict__ pkeys, int64_t np, int kind,
+                                                         uint64_t lo, uint64_t hi,
+                                                         const uint32_t* __restrict__ slot_row,
+                                                         unsigned long long* __restrict__ tstate,
+                                                         unsigned* __restrict__ ticket, int64_t ntiles,
+                                                         int64_t* __restrict__ total_out, int* __restrict__ err,
+                                                         join_out o) {
+    __shared__ int64_t sm[JP_NT / 32 + 1];
+    __shared__ int64_t s_tile, s_excl;
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int64_t row0 = tile * (int64_t)JP_TILE + warp * 32 * JP_IPT + lane;
+    uint32_t m[JP_IPT];
+    dense_lookup<KW>(pkeys, np, kind, lo, hi, slot_row, row0, m);
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) c += m[k] != NO_ROW;
+    int64_t wtot = dev_::warp_sum((int64_t)c);
+    int64_t total;
+    int64_t wbase = dev_::block_exclusive_sum<JP_NT, int64_t>(lane == 0 ? wtot : 0, sm, &total);
+    if (warp == 0) {
+        int64_t excl = lookback(tstate, tile, total, err);
+        __syncwarp();  // orders the lanes' acquire loads before lane 0 reads the error flag
+        if (lane == 0) {
+            s_excl = excl;
+            s_skip = *(volatile int*)err;
+            if (tile == ntiles - 1) *total_out = excl + total;
+        }
+    }
+    __syncthreads();
+    if (s_skip) return;  // block-uniform
+    wbase = __shfl_sync(0xffffffffu, wbase, 0) + s_excl;
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) {
+        bool hit = m[k] != NO_ROW;
+        unsigned bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            int64_t pos = wbase + __popc(bal & lt);
+            int64_t i = row0 + k * 32;
+            if (pos < np) {  // capacity bound (a unique-key probe never exceeds it)
+                if (o.key) st_w(o.key, o.key_width, pos, ld_w(pkeys, o.key_width, i));
+                for (int cc = 0; cc < o.n_pay; ++cc) {
+                    uint64_t v;
+                    switch (o.src[cc]) {
+                        case 1: v = ld_w(o.col[cc], o.width[cc], (int64_t)m[k]); break;
+                        case 2: v = ld_w(o.col[cc], o.width[cc], i); break;
+                        case 3: v = (uint64_t)m[k]; break;
+                        default: v = (uint64_t)i; break;
+                    }
+                    st_w(o.out[cc], o.width[cc], pos, v);
+                }
+            }
+        }
+        wbase += __popc(bal);
+    }
+}
+
 struct join_inputs {
     col lkey, rkey;
     std::vector<col> lpay, rpay;
@@ -352,27 +473,27 @@ struct join_inputs {
 // Output columns of a join: [key, left payloads.., right payloads..] or the
 // row-id pair; `dense` selects the source codes of the dense path.
 static join_out make_outputs(const join_inputs& in, bool build_left, bool rowids_only, bool pay_in_run, bool dense,
-                             int64_t total, cudaStream_t s, gx_table* out) {
+                             int64_t total, cudaStream_t s, gx_table* out, int64_t cap = -1) {
     join_out o;
     std::memset(&o, 0, sizeof(o));
     out->cols.clear();
     const int kw = size_of(in.lkey.type);
     if (rowids_only) {
-        out->cols.push_back(make_col(GX_INT64, total, s));
-        out->cols.push_back(make_col(GX_INT64, total, s));
+        out->cols.push_back(make_col(GX_INT64, total, s, cap));
+        out->cols.push_back(make_col(GX_INT64, total, s, cap));
         o.n_pay = 2;
         o.out[0] = out->cols[0].buf.get(); o.width[0] = 8; o.src[0] = build_left ? 3 : 4;
         o.out[1] = out->cols[1].buf.get(); o.width[1] = 8; o.src[1] = build_left ? 4 : 3;
         return o;
     }
-    out->cols.push_back(make_col(in.lkey.type, total, s));
+    out->cols.push_back(make_col(in.lkey.type, total, s, cap));
     o.key = out->cols[0].buf.get();
     o.key_width = kw;
     auto add_side = [&](bool is_build, const std::vector<col>& pays) {
         for (size_t c = 0; c < pays.size(); ++c) {
             int w = size_of(pays[c].type);
             require(w > 0, "join: STRING payload columns are not supported");
-            out->cols.push_back(make_col(pays[c].type, total, s));
+            out->cols.push_back(make_col(pays[c].type, total, s, cap));
             int j = o.n_pay++;
             o.out[j] = out->cols.back().buf.get();
             o.width[j] = w;
@@ -405,6 +526,42 @@ static bool dense_join(const join_inputs& in, const gx_join_hint& hint, bool row
     }
     if (read_scalar(flag.get<int>(), s)) return false;
     int64_t ntiles = ceil_div(std::max<int64_t>(np, 1), JP_TILE);
+    static const bool two_pass = getenv("GX_JOIN_TWO_PASS") != nullptr;
+    if (np > 0 && !two_pass) {
+        // Unique build keys: at most np matches, so the outputs are allocated
+        // up front and the probe runs once.
+        dbuf tstate((size_t)ntiles * 8 + 16, s), scal(16, s);
+        GX_CUDA(cudaMemsetAsync(tstate.get(), 0, (size_t)ntiles * 8 + 16, s));
+        GX_CUDA(cudaMemsetAsync(scal.get(), 0, 16, s));
+        join_out o = make_outputs(in, build_left, rowids_only, false, true, np, s, out, np);
+        unsigned* ticket = reinterpret_cast<unsigned*>(tstate.get<char>() + (size_t)ntiles * 8);
+        int64_t* total_out = scal.get<int64_t>();
+        int* err = reinterpret_cast<int*>(scal.get<char>() + 8);
+        {
+            GX_PROF("join_probe_write", s);
+            if (kw == 4)
+                k_dense_probe1<4><<<(unsigned)ntiles, JP_NT, 0, s>>>(pkey.data, np, kind, lo, hi, slot_row.get<uint32_t>(),
+                                                                     tstate.get<unsigned long long>(), ticket, ntiles,
+                                                                     total_out, err, o);
+            else
+                k_dense_probe1<8><<<(unsigned)ntiles, JP_NT, 0, s>>>(pkey.data, np, kind, lo, hi, slot_row.get<uint32_t>(),
+                                                                     tstate.get<unsigned long long>(), ticket, ntiles,
+                                                                     total_out, err, o);
+            GX_LAUNCHED();
+        }
+        int64_t hs[2];
+        GX_CUDA(cudaMemcpyAsync(hs, scal.get(), 16, cudaMemcpyDeviceToHost, s));
+        GX_CUDA(cudaStreamSynchronize(s));
+        if ((int)hs[1] == 0) {
+            const int64_t total = hs[0];
+            if (hint.max_out > 0 && total > hint.max_out)
+                fail(GX_EOVERFLOW, "join output (" + std::to_string(total) + " rows) exceeds hint.max_out (" +
+                                       std::to_string(hint.max_out) + ")");
+            for (auto& c : out->cols) c.size = total;
+            return true;
+        }
+        out->cols.clear();  // a look-back wait gave up: redo with the two-pass probe
+    }
     dbuf tc(ntiles * 8, s), toff((ntiles + 1) * 8, s);
     int64_t total = 0;
     if (np > 0) {

@@ -61,9 +61,9 @@ def make_instance(inst: dict):
     k = torch.empty(rows, dtype=kdt, device="cuda")
     cdf = None
     if inst["zipf"] > 0.01 and G > 1:
-        cdf = torch.from_numpy(gx.zipf_cdf(G, inst["zipf"])).cuda()
-        spec = gx.gen_spec(seed=inst["seed"], dist=gx.DIST_ZIPF, groups=G, zipf_s=inst["zipf"], scatter=1,
-                           zipf_cdf=cdf.data_ptr())
+        # Closed-form Zipf on the device: a CDF table of up to 2^28 entries
+        # would cost seconds per instance to build and to search.
+        spec = gx.gen_spec(seed=inst["seed"], dist=gx.DIST_ZIPF_APPROX, groups=G, zipf_s=inst["zipf"], scatter=1)
     else:
         spec = gx.gen_spec(seed=inst["seed"], groups=G, scatter=1)
     gx.generate_keys(k, spec)
@@ -90,34 +90,79 @@ def time_call(fn, reps: int = 1) -> float:
     return (time.perf_counter() - t0) / reps * 1e3
 
 
-def collect(instances: list[dict], fanout_every: int = 2, log=print) -> dict:
-    """Features and plain-engine timings (ms) of every variant per instance."""
+def heuristic_algo(key) -> int:
+    """The plain AUTO rule (what gx_groupby picks without the selector):
+    HASH when the full-column HyperLogLog estimate is at most 2^14 distinct
+    keys for 4-byte keys or 2^18 for 8-byte keys, else PARTITION
+    (src/cuda/operators/groupby/groupby.cu:68-119)."""
+    gx = _gx()
+    est = gx.compute_ndv_approx(key)
+    thr = (1 << 14) if key.element_size() == 4 else (1 << 18)
+    return gx.HASH if est <= thr else gx.PARTITION
+
+
+def _pack(instances, feats, times, ftimes, heur) -> dict:
+    return {"features": np.array(feats, np.float32).reshape(-1, F), "times": np.array(times, np.float64).reshape(-1, NV),
+            "fanout_times": np.array(ftimes, np.float64).reshape(-1, len(FANOUTS)),
+            "heuristic": np.array(heur, np.int32), "instances": json.dumps(instances[:len(feats)])}
+
+
+def collect(instances: list[dict], fanout_every: int = 4, log=None, out: str | None = None,
+            save_every: int = 128) -> dict:
+    """Features and plain-engine timings (ms) of every variant per instance.
+    With `out`, the rows collected so far are saved every `save_every`
+    instances, and a run resumes from an existing file."""
     import torch
     gx = _gx()
+    log = log or (lambda m: print(m, flush=True))
     reqs = [(0, gx.SUM), (0, gx.COUNT_ALL)]
     feats, times, ftimes, heur = [], [], [], []
+    if out and Path(out).exists():
+        d = np.load(out)
+        feats, times = list(d["features"]), list(d["times"])
+        ftimes, heur = list(d["fanout_times"]), list(d["heuristic"])
+        log(f"resuming after {len(feats)} instances")
+    phase = {"make": 0.0, "features": 0.0, "variants": 0.0, "fanouts": 0.0, "heuristic": 0.0}
+
+    def clock(name, t0):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        phase[name] += t1 - t0
+        return t1
+
     for idx, inst in enumerate(instances):
+        if idx < len(feats):
+            continue
+        t0 = time.perf_counter()
         k, v, cdf = make_instance(inst)
+        t0 = clock("make", t0)
         feats.append(features(k))
+        t0 = clock("features", t0)
         row = []
         for algo in (gx.HASH, gx.SORT, gx.PARTITION):
             row.append(time_call(lambda: gx.groupby([k], [v], reqs, gx.make_hint(algo))))
         times.append(row)
+        t0 = clock("variants", t0)
         fr = [np.nan] * len(FANOUTS)
         if idx % fanout_every == 0:
             for j, bits in enumerate(FANOUTS):
                 fr[j] = time_call(lambda: gx.groupby([k], [v], reqs, gx.make_hint(gx.PARTITION, radix_bits=bits)))
         ftimes.append(fr)
-        h = gx.make_hint(gx.AUTO_ALGO)
-        gx.groupby([k], [v], reqs, h)
-        heur.append(h.groupby_algo)
+        t0 = clock("fanouts", t0)
+        heur.append(heuristic_algo(k))
+        clock("heuristic", t0)
         del k, v, cdf
-        if idx % 256 == 0:
+        if (idx + 1) % 16 == 0:
+            log(f"{idx + 1} at {time.strftime('%H:%M:%S')}: " + " ".join(f"{n}={s:.1f}s" for n, s in phase.items()))
+        if (idx + 1) % save_every == 0:
             torch.cuda.empty_cache()
-            log(f"collected {idx + 1}/{len(instances)}")
-    return {"features": np.array(feats, np.float32), "times": np.array(times, np.float64),
-            "fanout_times": np.array(ftimes, np.float64), "heuristic": np.array(heur, np.int32),
-            "instances": json.dumps(instances)}
+            log(f"collected {idx + 1}/{len(instances)} at {time.strftime('%H:%M:%S')}")
+            if out:
+                np.savez(out, **_pack(instances, feats, times, ftimes, heur))
+    data = _pack(instances, feats, times, ftimes, heur)
+    if out:
+        np.savez(out, **data)
+    return data
 
 
 def targets_from(times: np.ndarray, ftimes: np.ndarray):
@@ -217,10 +262,10 @@ def main() -> None:
     t.add_argument("--epochs", type=int, default=3000)
     t.add_argument("--out", default=str(WEIGHTS))
     t.add_argument("--report", default=None)
+    t.add_argument("--heldout-out", default=None, help="save the held-out features / timings (for tests)")
     a = ap.parse_args()
     if a.cmd == "collect":
-        data = collect(draw_instances(a.instances, a.seed))
-        np.savez(a.out, **data)
+        collect(draw_instances(a.instances, a.seed), out=a.out)
         return
     d = np.load(a.timings)
     x, times, ft = d["features"], d["times"], d["fanout_times"]
@@ -244,6 +289,8 @@ def main() -> None:
     print(json.dumps(report))
     if a.report:
         Path(a.report).write_text(json.dumps(report, indent=1))
+    if a.heldout_out:
+        np.savez(a.heldout_out, features=x[ntr:], times=times[ntr:], heuristic=d["heuristic"][ntr:])
 
 
 if __name__ == "__main__":

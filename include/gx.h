@@ -63,8 +63,9 @@ typedef enum gx_sort_order { GX_ASCENDING = 0, GX_DESCENDING = 1 } gx_sort_order
  * Column view: mirrors gamax::column_view{data, size, type, offset}
  * (src/cuda/memory/column.hpp:13-94).  `size` is the number of visible rows
  * and element i lives at (char*)data + (offset + i) * size_of(type).
- * For GX_STRING the view's `data` points to a gx_string_columns struct
- * (ARROW layout: chars + int64 offsets of length rows+1,
+ * For GX_STRING the view's `data` points to a gx_string_columns struct in
+ * host memory holding device pointers (ARROW layout: chars + int64 offsets
+ * of length rows+1; the view's offset skips rows of the offsets array,
  * src/cuda/string/string_column.hpp:22-90).
  */
 typedef struct gx_column_view {
@@ -371,8 +372,10 @@ gx_status gx_dictionary_encode_with_order(gx_column_view col, int32_t encode_typ
 gx_status gx_dictionary_encode_with_dict(gx_column_view col, gx_column_view dict,
                                          int32_t encode_type, gx_stream_t stream,
                                          gx_column* out);
-/* String hash encode over an ARROW string column: dense int32 codes and the
- * dictionary's distinct strings in code order (chars + offsets). */
+/* String hash encode over an ARROW string column (a GX_STRING view): int32
+ * codes dense in [0, NDV), in first-insert order like the numeric hash
+ * encode; *dict_size = NDV.  The reference's dictionary_encode rejects
+ * STRING (dictionary_encode.cu:32-34); this is its string counterpart. */
 gx_status gx_dictionary_encode_strings(gx_column_view col, int64_t dictionary_size_hint,
                                        gx_stream_t stream, gx_column* codes,
                                        int64_t* dict_size);
@@ -394,7 +397,9 @@ typedef enum gx_key_dist {
     GX_DIST_UNIFORM = 0,  /* iid uniform rank in [0, G) */
     GX_DIST_CYCLIC = 1,   /* rank = bijective_shuffle(i) mod G: exactly N/G per key */
     GX_DIST_ZIPF = 2,     /* P(rank r) ∝ 1/(r+1)^s via inverse CDF */
-    GX_DIST_SEQUENCE = 3  /* rank = i */
+    GX_DIST_SEQUENCE = 3, /* rank = i */
+    GX_DIST_ZIPF_APPROX = 4 /* Zipf by the closed-form inverse of the continuous
+                               CDF, no table; device only (training data) */
 } gx_key_dist;
 
 typedef struct gx_gen_spec {

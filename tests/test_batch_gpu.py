@@ -40,3 +40,36 @@ def test_distinct_overflow_is_reported():
     plan = B.Plan(insts, max_distinct=100)
     with pytest.raises(gx.GxError):
         plan.run()
+
+
+@pytest.mark.parametrize("size_hint", [0, 16])
+def test_string_dictionary_encode_is_a_dense_bijection(size_hint):
+    import numpy as np
+    import torch
+    dchars, doffs = B.make_dictionary(500, seed=21)
+    d_dchars, d_doffs = torch.from_numpy(dchars).cuda(), torch.from_numpy(doffs).cuda()
+    rows = 100_003
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    src = torch.randint(0, 400, (rows,), device="cuda", dtype=torch.int32, generator=g)  # 400 of 500 used
+    offs = torch.zeros(rows + 1, dtype=torch.int64, device="cuda")
+    torch.cumsum((d_doffs[1:] - d_doffs[:-1])[src.long()], 0, out=offs[1:])
+    chars = torch.empty(int(offs[-1].item()), dtype=torch.uint8, device="cuda")
+    gx.check(gx.lib.gx_generate_strings(d_dchars.data_ptr(), d_doffs.data_ptr(), 500, src.data_ptr(), rows,
+                                        offs.data_ptr(), chars.data_ptr(), None))
+    skip = 3  # a view that starts at row 3
+    codes, ndv = gx.dictionary_encode_strings(chars, offs, row_offset=skip, size_hint=size_hint)
+    s, c = src.cpu().numpy()[skip:], codes.cpu().numpy()
+    assert len(c) == rows - skip and ndv == len(np.unique(s))
+    assert c.min() == 0 and c.max() == ndv - 1 and len(np.unique(c)) == ndv
+    # the same string <-> the same code, both ways
+    pairs = np.unique(np.stack([s, c], 1), axis=0)
+    assert len(pairs) == ndv
+
+
+def test_string_dictionary_encode_empty():
+    import torch
+    offs = torch.zeros(1, dtype=torch.int64, device="cuda")
+    chars = torch.zeros(1, dtype=torch.uint8, device="cuda")
+    codes, ndv = gx.dictionary_encode_strings(chars, offs)
+    assert codes.numel() == 0 and ndv == 0

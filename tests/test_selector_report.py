@@ -1,0 +1,59 @@
+"""The committed selector weights against the held-out instances, on the CPU.
+
+eiger_b200/selector_weights.npz holds the FP16 network trained on the GPU
+(python -m eiger_b200.selector train ...); tests/golden/selector_heldout.npz
+holds the 1024 held-out instances' sample features and the plain engine's
+measured time of every variant.  The NumPy restatement of the forward pass
+(oracle/mlp.py) scores them here: the learned choice must stay within 10%
+mean regret of the per-instance best variant and must beat the plain NDV rule
+the reference uses (src/cuda/operators/groupby/groupby.cu:68-119)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import mlp as M
+
+ROOT = Path(__file__).resolve().parents[1]
+WEIGHTS = ROOT / "eiger_b200" / "selector_weights.npz"
+HELDOUT = ROOT / "tests" / "golden" / "selector_heldout.npz"
+HASH, PARTITION = 1, 5  # gx_groupby_algo values
+
+
+def regret(times, choice):
+    best = times.min(axis=1)
+    return float(np.mean(times[np.arange(len(choice)), choice] / best - 1.0))
+
+
+@pytest.fixture(scope="module")
+def data():
+    if not (WEIGHTS.exists() and HELDOUT.exists()):
+        pytest.skip("selector weights or held-out set not committed")
+    w, h = np.load(WEIGHTS), np.load(HELDOUT)
+    return w, h
+
+
+def test_learned_choice_regret_and_gain_over_plain_rule(data):
+    w, h = data
+    params = w["params"].view(np.float16).astype(np.float64)
+    x = (h["features"] - w["mean"]) / w["std"]
+    scores = M.forward(params, x.astype(np.float64))
+    learned = np.argmin(scores[:, :3], axis=1)
+    times = h["times"]
+    heur = np.where(h["heuristic"] == HASH, 0, 2)
+    r_learned, r_heur = regret(times, learned), regret(times, heur)
+    assert len(times) >= 1024
+    assert r_learned <= 0.10, r_learned
+    assert r_learned < r_heur, (r_learned, r_heur)
+
+
+def test_report_matches_recomputation(data):
+    import json
+    w, h = data
+    meta = json.loads(str(w["meta"]))
+    params = w["params"].view(np.float16).astype(np.float64)
+    x = (h["features"] - w["mean"]) / w["std"]
+    learned = np.argmin(M.forward(params, x)[:, :3], axis=1)
+    # the GPU forward (FP16 weights, FP32 accumulation) and this float64 one
+    # may split a near-tie differently on a few instances
+    assert abs(regret(h["times"], learned) - meta["regret_learned"]) < 0.02
