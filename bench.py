@@ -1,7 +1,8 @@
 #!/usr/bin/env python
 """Benchmark of the relational operator core on B200.
 
-Default workload (one "step"): hash group-by over 2^28 rows — int32 keys
+Default workload (one "step"): group-by over 2^28 rows (variant chosen by the
+engine's plain AUTO rule unless --algo names one) — int32 keys
 (scattered, uniform over --groups distinct values), an int64 column uniform
 in [0, 2^31) and a float64 column uniform in [0, 1), SUM / COUNT / MIN / MAX
 on both value columns (the group-by sweep configuration, one point of it).
@@ -174,11 +175,14 @@ def run_gx(args) -> None:
     # ----------------------------------------------------------- group-by
     k, iv, fv = make_groupby_inputs(gx, torch, rows, G, seed=42 + rank)
     reqs = groupby_reqs(gx)
-    hint_algo = {"hash": gx.HASH, "sort": gx.SORT, "partition": gx.PARTITION}[args.algo]
+    hint_algo = {"auto": gx.AUTO_ALGO, "hash": gx.HASH, "sort": gx.SORT, "partition": gx.PARTITION}[args.algo]
+    chosen = {}
 
     def step():
         h = gx.make_hint(hint_algo, G)
-        return gx.groupby([k], [iv, fv], reqs, h)
+        t = gx.groupby([k], [iv, fv], reqs, h)
+        chosen["algo"], chosen["radix_bits"] = h.groupby_algo, h.radix_bits
+        return t
 
     res = step()
     ngroups = res.num_rows
@@ -190,19 +194,29 @@ def run_gx(args) -> None:
         ms = time_steps(torch, step, args.steps, args.warmup, dist)
     gx.lib.gx_profile_enable(0)
     launches = gx.kernel_launches() - launches0
-    main_kernel = {"hash": "hash_groupby", "sort": "segmented_reduce", "partition": "partition_aggregate"}[args.algo]
-    kms, kcnt = kernel_ms(gx, main_kernel)
-    gx.lib.gx_profile_reset()
-    ms_step = ms / args.steps
-    value = world * rows / (ms_step * 1e-3) / 1e6
     in_bytes = rows * (4 + 8 + 8)
     out_bytes = ngroups * (4 + 8 * 7)
-    # The kernel's per-launch algorithmic bytes: key + value columns once.
+    # Per-launch algorithmic bytes of each timed kernel: the key and value
+    # columns read once (aggregation kernels), read and written once per
+    # radix pass (partition scatter).
+    kernel_bytes = {"hash_groupby": in_bytes, "partition_aggregate": in_bytes, "segmented_reduce": in_bytes,
+                    "partition_scatter": 2 * in_bytes, "radix_scatter": 2 * in_bytes}
+    kstats = {name: kernel_ms(gx, name) for name in kernel_bytes}
+    gx.lib.gx_profile_reset()
+    main_kernel = max(kstats, key=lambda nm: kstats[nm][0])
+    prof_steps = args.steps + args.warmup  # profiling covers the warm-up steps too
+    kms, kcnt = kstats[main_kernel]
+    ms_step = ms / args.steps
+    value = world * rows / (ms_step * 1e-3) / 1e6
     k_launch_ms = kms / max(kcnt, 1)
-    achieved = in_bytes / (k_launch_ms * 1e-3) / 1e9 if kcnt else None
+    achieved = kernel_bytes[main_kernel] / (k_launch_ms * 1e-3) / 1e9 if kcnt else None
+    algo_name = {gx.HASH: "hash", gx.SORT: "sort", gx.SORT_OPT: "sort_opt", gx.SORT_GFUR: "sort_gfur",
+                 gx.PARTITION: "partition", gx.PARTITION_GFUR: "partition_gfur"}.get(chosen.get("algo"), "?")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": args.traffic,
-                "kernel": main_kernel, "kernel_ms": k_launch_ms, "peak_source": peaks["source"],
+                "kernel": main_kernel, "kernel_ms": k_launch_ms, "launches_per_step": kcnt / prof_steps,
+                "kernel_share_of_step": kms / prof_steps / max(ms_step, 1e-9), "peak_source": peaks["source"],
+                "kernels_ms_per_step": {nm: round(t / prof_steps, 4) for nm, (t, c) in kstats.items() if c},
                 "operator_frac": (in_bytes + out_bytes) / (ms_step * 1e-3) / 1e9 / peaks["hbm_gbs"]}
 
     # ------------------------------------------------------------- e2e
@@ -312,9 +326,11 @@ def run_gx(args) -> None:
             "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
-            "config": {"workload": f"hash group-by, {rows} rows, int32 keys uniform over {G} scattered values, "
-                                   "int64 [0,2^31) + float64 [0,1) values, SUM/COUNT/MIN/MAX on both",
+            "config": {"workload": f"group-by ({args.algo}: ran {algo_name}), {rows} rows, int32 keys uniform over "
+                                   f"{G} scattered values, int64 [0,2^31) + float64 [0,1) values, "
+                                   "SUM/COUNT/MIN/MAX on both",
                        "rows": rows, "groups": G, "groups_found": ngroups, "algo": args.algo,
+                       "variant_run": algo_name, "radix_bits": chosen.get("radix_bits"),
                        "l2": "inputs (5.4 GB) larger than L2; no flush"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk.summary(), "join": join, "batched": batched,
@@ -436,7 +452,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=["gx", "reference"], default="gx")
     ap.add_argument("--rows", type=int, default=1 << 28)
     ap.add_argument("--groups", type=int, default=1 << 16)
-    ap.add_argument("--algo", choices=["hash", "sort", "partition"], default="hash")
+    ap.add_argument("--algo", choices=["auto", "hash", "sort", "partition"], default="auto",
+                    help="group-by variant (auto: the engine's plain selection rule)")
     ap.add_argument("--join-rows", type=int, default=1 << 28)
     ap.add_argument("--no-join", action="store_true")
     ap.add_argument("--batch-instances", type=int, default=512, help="batched pipeline instances (0: skip)")

@@ -259,7 +259,9 @@ class Table:
         self.handle = C.c_void_p(handle)
 
     def __del__(self):
-        if getattr(self, "handle", None) and self.handle.value:
+        # At interpreter exit the module globals may already be gone; the
+        # process teardown releases the device memory then.
+        if getattr(self, "handle", None) and self.handle.value and lib is not None:
             lib.gx_table_free(self.handle)
             self.handle = C.c_void_p(0)
 

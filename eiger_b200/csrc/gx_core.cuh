@@ -32,6 +32,11 @@ struct error : std::runtime_error {
 inline void require(bool ok, const std::string& msg) {
     if (!ok) fail(GX_EINVAL, msg);
 }
+// Longest linear-probe walk in a global hash table.  Tables run at load
+// <= 1/2, where walks are a few slots long; a walk this long means the table
+// is (nearly) full, so the kernel reports overflow and the host retries with
+// a larger table instead of scanning the whole table for every row.
+constexpr uint64_t GX_PROBE_LIMIT = 4096;
 // Sets the calling thread's gx_last_error_message (gx_capi.cu).
 void set_last_error(const char* msg);
 

@@ -61,7 +61,7 @@ __device__ __forceinline__ int64_t d_find(const dtable& t, uint64_t k, bool inse
         return t.keys[s] == EMPTY ? s : -1;
     }
     uint64_t slot = dhash<KW>(k) & t.mask;
-    for (uint64_t p = 0; p <= t.mask; ++p) {
+    for (uint64_t p = 0, lim = t.mask < GX_PROBE_LIMIT ? t.mask : GX_PROBE_LIMIT - 1; p <= lim; ++p) {
         unsigned long long cur = ((volatile unsigned long long*)t.keys)[slot];
         if (cur == k) return (int64_t)slot;
         if (cur == EMPTY) {

@@ -8,6 +8,21 @@ namespace gx {
 // ----- hash group-by (gx_groupby_hash.cu) -----
 void init_records(uint64_t* recs, int64_t nrec, const agg_desc& d, uint64_t empty, cudaStream_t s);
 int hash_smem_slots(const agg_desc& d, int key_width, int64_t groups_bound, int* replicas);
+// A work unit of radix-partitioned rows: rows [begin, end) of one partition;
+// split = the partition is spread over several units.
+struct part_unit {
+    int64_t begin, end;
+    int split, pad;
+};
+// Aggregates partitioned rows unit by unit in shared-memory tables (the hash
+// group-by's table code); `shift` = partition bits of the key hash, gpp =
+// expected groups per partition.  Final groups of whole, unspilled units are
+// appended to orec / *ocount; the rest merge into the global record table
+// grec (gcap records + the sentinel record; gflags[0] sentinel, [1] overflow).
+// Returns false when the groups per partition do not fit a shared table.
+bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d, const part_unit* units,
+                          const int64_t* n_units, int64_t gpp, int shift, uint64_t* grec, uint64_t gcap, int* gflags,
+                          uint64_t* orec, unsigned long long* ocount, int64_t rec_cap, int* rec_ovf, cudaStream_t s);
 void hash_groupby(const col& key, const agg_plan& p, gx_groupby_hint* hint, cudaStream_t s,
                   gx_table* out);
 

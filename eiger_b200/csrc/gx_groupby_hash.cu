@@ -51,7 +51,7 @@ __device__ __forceinline__ uint64_t* g_find_or_insert(const gtable& t, const agg
         return t.recs + (t.mask + 1) * d.rec_words;
     }
     uint64_t slot = h & t.mask;
-    for (uint64_t p = 0; p <= t.mask; ++p) {
+    for (uint64_t p = 0, lim = t.mask < GX_PROBE_LIMIT ? t.mask : GX_PROBE_LIMIT - 1; p <= lim; ++p) {
         uint64_t* r = t.recs + slot * d.rec_words;
         uint64_t cur = *(volatile uint64_t*)r;
         if (cur == kw) return r;
@@ -191,11 +191,18 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restri
         }
 #pragma unroll
         for (int u = 0; u < HGB_UNROLL; ++u) {
-            int64_t i = base + u * HGB_NT + threadIdx.x;
-            if (i >= n) continue;
-            uint32_t h = key_hash<KW>(kw[u]);
+            const int64_t i = base + u * HGB_NT + threadIdx.x;
+            const bool valid = i < n;
+            uint32_t h = 0;
             int slot = -1;
-            if (SMEM) slot = s_find_or_insert<KW>(st, kw[u], h);
+            if (valid) {
+                h = key_hash<KW>(kw[u]);
+                if (SMEM) slot = s_find_or_insert<KW>(st, kw[u], h);
+            }
+            // Lanes leave the probe loop at different steps; regroup the warp
+            // so the updates below issue once per warp, not once per exit step.
+            __syncwarp();
+            if (!valid) continue;
             if (slot >= 0) {
                 // The per-replica count is kept even without COUNT: it tells
                 // the merge which replicas saw the group (for ANY).
@@ -236,6 +243,172 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restri
                 dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], x);
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Aggregation of radix-partitioned rows, one work unit at a time.  A unit is
+// a row range of one partition, so it holds only that partition's groups and
+// the CTA's shared table (sized for them) absorbs every row; the shared-table
+// update is the same code as k_hash_groupby's.  The table slot comes from the
+// hash bits above the partition bits.  A unit that is a whole partition and
+// never overflowed its table appends its final groups densely; a split (or
+// spilled) unit merges into the global table like k_hash_groupby's CTAs.
+// ---------------------------------------------------------------------------
+template <int KW, int NV, class... ACCS>
+__global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict__ keys, int key_kind, agg_desc d,
+                                                           const part_unit* __restrict__ units,
+                                                           const int64_t* __restrict__ n_units, uint32_t s_slots,
+                                                           int reps, int shift, gtable g,
+                                                           uint64_t* __restrict__ out_recs,
+                                                           unsigned long long* __restrict__ out_count,
+                                                           int64_t rec_cap, int* __restrict__ rec_ovf) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_fill, s_spill;
+    __shared__ unsigned long long s_base;
+    __shared__ int64_t scan_sm[HGB_NT / 32 + 1];
+    using kt = typename stable<KW>::kt;
+    const kt EMPTY = KW == 4 ? (kt)S_EMPTY4 : (kt)S_EMPTY8;
+    stable<KW> st;
+    const size_t S = s_slots;
+    const size_t key_bytes = (S * KW + 15) & ~size_t(15);
+    st.keys = reinterpret_cast<kt*>(smem);
+    st.counts = reinterpret_cast<unsigned*>(smem + key_bytes);
+    st.acc = reinterpret_cast<uint64_t*>(smem + key_bytes + ((S * 4 * reps + 15) & ~size_t(15)));
+    st.fill = &s_fill;
+    st.mask = s_slots - 1;
+    st.limit = (int)(s_slots / 2);
+    st.S = s_slots;
+    st.R = reps;
+    const int rep = (int)(threadIdx.x % (unsigned)reps);
+    unsigned* my_counts = st.counts + (size_t)rep * S;
+    uint64_t* my_acc = st.acc + (size_t)rep * d.n_acc * S;
+    const int64_t nu = *n_units;
+    for (int64_t u = blockIdx.x; u < nu; u += gridDim.x) {
+        const part_unit un = units[u];
+        for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) st.keys[i] = EMPTY;
+        for (uint32_t i = threadIdx.x; i < s_slots * reps; i += HGB_NT) st.counts[i] = 0;
+        for (int r = 0; r < reps; ++r)
+            for (int a = 0; a < d.n_acc; ++a) {
+                const uint64_t idv = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
+                uint64_t* base = st.acc + ((size_t)r * d.n_acc + a) * S;
+                for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) base[i] = idv;
+            }
+        if (threadIdx.x == 0) { s_fill = 0; s_spill = 0; }
+        __syncthreads();
+        const int64_t tile = (int64_t)HGB_NT * HGB_UNROLL;
+        for (int64_t base = un.begin; base < un.end; base += tile) {
+            uint64_t kw[HGB_UNROLL];
+            uint64_t v[HGB_UNROLL][NV];
+#pragma unroll
+            for (int q = 0; q < HGB_UNROLL; ++q) {
+                const int64_t i = base + q * HGB_NT + threadIdx.x;
+                if (i < un.end) {
+                    if (KW == 4) kw[q] = canon32(__ldg(static_cast<const unsigned*>(keys) + i), key_kind);
+                    else kw[q] = canon64(__ldg(static_cast<const unsigned long long*>(keys) + i), key_kind);
+                    if constexpr (sizeof...(ACCS) > 0) {
+#pragma unroll
+                        for (int c = 0; c < NV; ++c)
+                            v[q][c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NV; ++c)
+                            if (c < d.n_cols) v[q][c] = dev_::load_lane(d.col_ptr[c], d.col_width[c], d.col_kind[c], i);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < HGB_UNROLL; ++q) {
+                const int64_t i = base + q * HGB_NT + threadIdx.x;
+                const bool valid = i < un.end;
+                uint32_t h = 0;
+                int slot = -1;
+                if (valid) {
+                    h = key_hash<KW>(kw[q]);
+                    slot = s_find_or_insert<KW>(st, kw[q], h >> shift);
+                }
+                __syncwarp();  // regroup after the probe loop (see k_hash_groupby)
+                if (!valid) continue;
+                if (slot >= 0) {
+                    atomicAdd(&my_counts[slot], 1u);
+                    if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, slot, v[q]);
+                    else dev_::shared_row_update<NV>(my_acc, s_slots, slot, d, v[q]);
+                } else {
+                    if (!s_spill) s_spill = 1;
+                    uint64_t* r = g_find_or_insert<KW>(g, d, kw[q], h);
+                    if (r) g_update(r, d, v[q], 1ull);
+                }
+            }
+        }
+        __syncthreads();
+        const bool final_groups = !un.split && !s_spill;
+        if (final_groups) {
+            if (threadIdx.x == 0) {
+                s_base = atomicAdd(out_count, (unsigned long long)s_fill);
+                if ((int64_t)(s_base + s_fill) > rec_cap) atomicExch(rec_ovf, 1);
+            }
+            __syncthreads();
+        }
+        if (final_groups && (int64_t)(s_base + s_fill) <= rec_cap) {
+            // Compact the occupied slots (slot order) into dense records.
+            int64_t running = 0;
+            for (uint32_t i0 = 0; i0 < s_slots; i0 += HGB_NT) {
+                const uint32_t i = i0 + threadIdx.x;
+                const bool live = i < s_slots && st.keys[i] != EMPTY;
+                int64_t tot;
+                const int64_t ex = dev_::block_exclusive_sum<HGB_NT, int64_t>(live ? 1 : 0, scan_sm, &tot);
+                if (live) {
+                    uint64_t* r = out_recs + (s_base + running + ex) * d.rec_words;
+                    unsigned long long c = 0;
+                    int first = -1;
+                    for (int rp = 0; rp < reps; ++rp) {
+                        const unsigned cr = st.counts[(size_t)rp * S + i];
+                        c += cr;
+                        if (cr && first < 0) first = rp;
+                    }
+                    r[0] = (uint64_t)st.keys[i];
+                    if (d.has_count) r[d.count_word] = c;
+                    for (int a = 0; a < d.n_acc; ++a) {
+                        uint64_t x = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
+                        if (first >= 0) {
+                            x = st.acc[((size_t)first * d.n_acc + a) * S + i];
+                            for (int rp = first + 1; rp < reps; ++rp)
+                                if (st.counts[(size_t)rp * S + i])
+                                    x = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], x,
+                                                          st.acc[((size_t)rp * d.n_acc + a) * S + i]);
+                        }
+                        r[d.acc_word0 + a] = x;
+                    }
+                }
+                running += tot;
+            }
+        } else if (!final_groups) {
+            for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) {
+                const kt k = st.keys[i];
+                if (k == EMPTY) continue;
+                const uint64_t kwv = (uint64_t)k;
+                uint64_t* r = g_find_or_insert<KW>(g, d, kwv, key_hash<KW>(kwv));
+                if (!r) continue;
+                unsigned long long c = 0;
+                int first = -1;
+                for (int rp = 0; rp < reps; ++rp) {
+                    const unsigned cr = st.counts[(size_t)rp * S + i];
+                    c += cr;
+                    if (cr && first < 0) first = rp;
+                }
+                if (first < 0) continue;
+                if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), c);
+                for (int a = 0; a < d.n_acc; ++a) {
+                    uint64_t x = st.acc[((size_t)first * d.n_acc + a) * S + i];
+                    for (int rp = first + 1; rp < reps; ++rp)
+                        if (st.counts[(size_t)rp * S + i])
+                            x = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], x,
+                                                  st.acc[((size_t)rp * d.n_acc + a) * S + i]);
+                    dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], x);
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -346,6 +519,54 @@ static void launch_hash(bool smem_mode, int nv, int grid, size_t smem, cudaStrea
 #undef GX_HL
 }
 
+// ---- partitioned units ----------------------------------------------------
+struct units_args {
+    const void* keys;
+    int kind;
+    const part_unit* units;
+    const int64_t* n_units;
+    uint32_t slots;
+    int reps, shift;
+    gtable g;
+    uint64_t* orec;
+    unsigned long long* ocount;
+    int64_t rec_cap;
+    int* rec_ovf;
+};
+
+template <int KW, int NV, class... ACCS>
+static void launch_units(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a) {
+    GX_CUDA(cudaFuncSetAttribute(k_hash_units<KW, NV, ACCS...>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    k_hash_units<KW, NV, ACCS...><<<grid, HGB_NT, smem, s>>>(a.keys, a.kind, d, a.units, a.n_units, a.slots, a.reps,
+                                                             a.shift, a.g, a.orec, a.ocount, a.rec_cap, a.rec_ovf);
+}
+
+template <int KW, int NV, class... ACCS>
+static bool try_units_spec(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a) {
+    if (d.n_cols != NV || !plan_matches<ACCS...>(d)) return false;
+    launch_units<KW, NV, ACCS...>(grid, smem, s, d, a);
+    return true;
+}
+
+template <int KW>
+static void units_dispatch(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a) {
+    using namespace spec;
+    if (!getenv("GX_HASH_GENERIC")) {
+        if (try_units_spec<KW, 1, A<OP_SUM, VK_I, 0>>(grid, smem, s, d, a)) return;
+        if (try_units_spec<KW, 1, A<OP_SUM, VK_F, 0>>(grid, smem, s, d, a)) return;
+        if (try_units_spec<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_MIN, VK_I, 0>, A<OP_MAX, VK_I, 0>, A<OP_SUM, VK_F, 1>,
+                           A<OP_MIN, VK_F, 1>, A<OP_MAX, VK_F, 1>>(grid, smem, s, d, a))
+            return;
+        if (try_units_spec<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_SUM, VK_I, 1>>(grid, smem, s, d, a)) return;
+    }
+    const int nv = d.n_cols <= 1 ? 1 : d.n_cols <= 2 ? 2 : d.n_cols <= 4 ? 4 : 8;
+    if (nv == 1) launch_units<KW, 1>(grid, smem, s, d, a);
+    else if (nv == 2) launch_units<KW, 2>(grid, smem, s, d, a);
+    else if (nv == 4) launch_units<KW, 4>(grid, smem, s, d, a);
+    else launch_units<KW, 8>(grid, smem, s, d, a);
+}
+
 // Runs the hash group-by into a global table of `cap` records.
 // Returns false when the table overflowed (caller retries larger).
 static bool hash_groupby_run(const col& key, int out_key_type, const agg_plan& p, uint64_t cap, int smem_mode,
@@ -416,6 +637,29 @@ void hash_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hint, c
         cap *= 4;
     }
     fail(GX_EOVERFLOW, "hash group-by table overflow after retries");
+}
+
+bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d, const part_unit* units,
+                          const int64_t* n_units, int64_t gpp, int shift, uint64_t* grec, uint64_t gcap, int* gflags,
+                          uint64_t* orec, unsigned long long* ocount, int64_t rec_cap, int* rec_ovf, cudaStream_t s) {
+    const size_t budget = 200 * 1024;
+    const size_t per_rep = 4 + 8 * (size_t)d.n_acc;
+    // Slots for the fullest partition expected (Poisson tail), at load <= 1/2.
+    const double gmax = (double)gpp + 4.0 * std::sqrt((double)gpp) + 8.0;
+    uint32_t slots = (uint32_t)next_pow2((uint64_t)std::max(64.0, 2.0 * gmax));
+    if ((size_t)slots * (kw + per_rep) > budget) return false;
+    size_t reps = (budget - (size_t)slots * kw) / ((size_t)slots * per_rep);
+    reps = std::max<size_t>(1, std::min<size_t>(32, reps));
+    const size_t smem = (((size_t)slots * kw + 15) & ~size_t(15)) + (((size_t)slots * 4 * reps + 15) & ~size_t(15)) +
+                        (size_t)slots * reps * 8 * d.n_acc;
+    units_args a{keys, kind, units, n_units, slots, (int)reps, shift,
+                 gtable{grec, gcap - 1, gflags, gflags + 1}, orec, ocount, rec_cap, rec_ovf};
+    const int grid = dev().sm_count;
+    GX_PROF("partition_aggregate", s);
+    if (kw == 4) units_dispatch<4>(grid, smem, s, d, a);
+    else units_dispatch<8>(grid, smem, s, d, a);
+    GX_LAUNCHED();
+    return true;
 }
 
 }  // namespace gx

@@ -157,6 +157,111 @@ __global__ void __launch_bounds__(PS_NT) k_part_scatter(const void* __restrict__
     }
 }
 
+// The same scatter for NC <= 3 columns with every column's values loaded into
+// registers up front, so all of a tile's global loads are in flight together
+// (the general kernel loads one column per staging round).
+template <int KW, int NC>
+__global__ void __launch_bounds__(PS_NT) k_part_scatter_r(const void* __restrict__ keys, int64_t n, int kind,
+                                                           int shift, int dbits, int64_t ntiles,
+                                                           const int64_t* __restrict__ offsets, move_cols mc) {
+    __shared__ unsigned whist[PS_WARPS * PS_BINS];
+    __shared__ int64_t gbase[PS_BINS];
+    __shared__ unsigned dbase[PS_BINS];
+    extern __shared__ __align__(16) unsigned long long part_dyn[];
+    unsigned long long* stage = part_dyn;                                          // [PS_TILE]
+    unsigned short* sdig = reinterpret_cast<unsigned short*>(part_dyn + PS_TILE);  // [PS_TILE]
+
+    const int bins = 1 << dbits;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < PS_WARPS * PS_BINS; i += PS_NT) whist[i] = 0;
+    const int64_t tile_base = blockIdx.x * (int64_t)PS_TILE;
+    const int tile_n = (int)min((int64_t)PS_TILE, n - tile_base);
+    unsigned long long x[NC][PS_IPT];
+#pragma unroll
+    for (int k = 0; k < PS_IPT; ++k) {
+        const int local = warp * 32 * PS_IPT + k * 32 + lane;
+        const int64_t i = tile_base + local;
+        const bool valid = local < tile_n;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            x[c][k] = 0;
+            if (valid) {
+                if (mc.iota[c]) x[c][k] = (unsigned long long)i;
+                else if (mc.width[c] == 8) x[c][k] = __ldg(static_cast<const unsigned long long*>(mc.in[c]) + i);
+                else x[c][k] = __ldg(static_cast<const unsigned*>(mc.in[c]) + i);
+            }
+        }
+    }
+    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned dig[PS_IPT], rank[PS_IPT];
+#pragma unroll
+    for (int k = 0; k < PS_IPT; ++k) {
+        const int local = warp * 32 * PS_IPT + k * 32 + lane;
+        const bool valid = local < tile_n;
+        uint64_t kb;
+        if (KW == 4) kb = canon32((uint32_t)x[0][k], kind);
+        else kb = canon64(x[0][k], kind);
+        const unsigned d = valid ? (part_hash<KW>(kb) >> shift) & (bins - 1) : 0xFFFFu;
+        dig[k] = d;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned r = __popc(peers & lt);
+        const unsigned prior = valid ? whist[warp * PS_BINS + d] : 0;
+        rank[k] = prior + r;
+        __syncwarp();
+        if (valid && r == 0) whist[warp * PS_BINS + d] = prior + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    if (threadIdx.x < PS_BINS) {
+        unsigned run = 0;
+        if ((int)threadIdx.x < bins)
+            for (int w = 0; w < PS_WARPS; ++w) {
+                const unsigned c = whist[w * PS_BINS + threadIdx.x];
+                whist[w * PS_BINS + threadIdx.x] = run;
+                run += c;
+            }
+        dbase[threadIdx.x] = run;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned v[PS_BINS / 32], s = 0;
+#pragma unroll
+        for (int j = 0; j < PS_BINS / 32; ++j) { v[j] = dbase[lane * (PS_BINS / 32) + j]; s += v[j]; }
+        unsigned run = dev_::warp_inclusive_sum(s) - s;
+#pragma unroll
+        for (int j = 0; j < PS_BINS / 32; ++j) { dbase[lane * (PS_BINS / 32) + j] = run; run += v[j]; }
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < bins)
+        gbase[threadIdx.x] = offsets[(int64_t)threadIdx.x * ntiles + blockIdx.x] - (int64_t)dbase[threadIdx.x];
+    unsigned pos[PS_IPT];
+#pragma unroll
+    for (int k = 0; k < PS_IPT; ++k) {
+        const int local = warp * 32 * PS_IPT + k * 32 + lane;
+        if (local < tile_n) {
+            pos[k] = dbase[dig[k]] + whist[warp * PS_BINS + dig[k]] + rank[k];
+            sdig[pos[k]] = (unsigned short)dig[k];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PS_IPT; ++k) {
+            const int local = warp * 32 * PS_IPT + k * 32 + lane;
+            if (local < tile_n) stage[pos[k]] = x[c][k];
+        }
+        __syncthreads();
+        const int w = mc.width[c];
+        for (int j = threadIdx.x; j < tile_n; j += PS_NT) {
+            const int64_t o = gbase[sdig[j]] + j;
+            if (w == 8) static_cast<unsigned long long*>(mc.out[c])[o] = stage[j];
+            else static_cast<unsigned*>(mc.out[c])[o] = (unsigned)stage[j];
+        }
+    }
+}
+
 // Work units: partition p split into ceil(size/T) units.
 __global__ void k_unit_counts(const int64_t* __restrict__ part_start, int P, int64_t T,
                               int64_t* __restrict__ ucount) {
@@ -166,7 +271,7 @@ __global__ void k_unit_counts(const int64_t* __restrict__ part_start, int P, int
         ucount[p] = sz == 0 ? 0 : (sz + T - 1) / T;
     }
 }
-struct unit { int64_t begin, end; int split; int pad; };
+using unit = part_unit;
 __global__ void k_unit_fill(const int64_t* __restrict__ part_start, const int64_t* __restrict__ uoff, int P,
                             int64_t T, unit* __restrict__ units) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -202,7 +307,7 @@ __device__ __forceinline__ uint64_t* pg_find(const pglobal& t, const agg_desc& d
         return t.recs + (t.mask + 1) * d.rec_words;
     }
     uint64_t slot = (h * 0x9E3779B1u) & t.mask;
-    for (uint64_t p = 0; p <= t.mask; ++p) {
+    for (uint64_t p = 0, lim = t.mask < GX_PROBE_LIMIT ? t.mask : GX_PROBE_LIMIT - 1; p <= lim; ++p) {
         uint64_t* r = t.recs + slot * d.rec_words;
         uint64_t cur = *(volatile uint64_t*)r;
         if (cur == kw) return r;
@@ -367,10 +472,14 @@ void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_
     static bool attr[16] = {};
     if (!attr[dev().device]) {
         GX_CUDA(cudaFuncSetAttribute(k_part_scatter<KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+        GX_CUDA(cudaFuncSetAttribute(k_part_scatter_r<KW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+        GX_CUDA(cudaFuncSetAttribute(k_part_scatter_r<KW, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
         attr[dev().device] = true;
     }
     GX_PROF("partition_scatter", s);
-    k_part_scatter<KW><<<(unsigned)ntiles, PS_NT, dyn, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc);
+    if (mc.n == 2) k_part_scatter_r<KW, 2><<<(unsigned)ntiles, PS_NT, dyn, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc);
+    else if (mc.n == 3) k_part_scatter_r<KW, 3><<<(unsigned)ntiles, PS_NT, dyn, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc);
+    else k_part_scatter<KW><<<(unsigned)ntiles, PS_NT, dyn, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc);
     GX_LAUNCHED();
 }
 
@@ -400,7 +509,12 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     int64_t bound = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
     if (!(hint->groups_upper_bound > 0 && hint->groups_upper_bound < n) && n > (1 << 16))
         bound = std::min<int64_t>(n, ndv_estimate(key, s) * 9 / 8 + 64);
-    int64_t gpp = 16;
+    // About 256 groups per partition: a shared table of ~1K slots holds them
+    // (with a few accumulator replicas), and up to 2^16 groups need a single
+    // 8-bit radix pass.
+    int64_t gpp = gfur ? 16 : 256;
+    for (int c = 0; c < d.n_cols; ++c)
+        if (d.col_width[c] < 4) gpp = 16;
     if (const char* e = getenv("GX_PART_GROUPS")) gpp = std::max<int64_t>(1, atoll(e));
     int R = hint->radix_bits;
     if (R <= 0) R = ilog2_ceil((uint64_t)std::max<int64_t>(1, ceil_div(bound, gpp)));
@@ -461,7 +575,7 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     // Split threshold: partitions above twice the mean size are split (Zipf
     // hot partitions), and with few partitions every partition is split so
     // that about four units per SM exist.
-    int64_t T = std::max<int64_t>(1 << 14, std::min<int64_t>(2 * ceil_div(n, P), ceil_div(n, (int64_t)dev().sm_count * 4)));
+    int64_t T = std::max<int64_t>(1 << 14, std::min<int64_t>(2 * ceil_div(n, P), ceil_div(n, (int64_t)dev().sm_count * 8)));
     dbuf ucount((size_t)P * 8, s), uoff((size_t)(P + 1) * 8, s);
     k_unit_counts<<<(unsigned)ceil_div(P, 256), 256, 0, s>>>(pstart.get<int64_t>(), P, T, ucount.get<int64_t>());
     GX_LAUNCHED();
@@ -478,7 +592,10 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     int64_t total_units = read_scalar(uoff.get<int64_t>() + P, s);
     int64_t live_parts = std::min<int64_t>(P, n);
     uint64_t gcap = 1u << 16;
-    if (total_units > live_parts) gcap = std::max<uint64_t>(gcap, next_pow2((uint64_t)bound * 2));
+    // Also when partitions hold more groups than a shared table (radix bits
+    // forced low by the hint): their overflow spills here.
+    if (total_units > live_parts || ceil_div(bound, (int64_t)P) > 512)
+        gcap = std::max<uint64_t>(gcap, next_pow2((uint64_t)bound * 2));
     int64_t out_cap = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
     // Output records: sized from the group bound, grown (up to n) on overflow.
     int64_t rec_cap = std::max<int64_t>(1, std::min<int64_t>(n, std::max<int64_t>(bound + bound / 4, 4096)));
@@ -491,7 +608,17 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
         unsigned long long* ocount = reinterpret_cast<unsigned long long*>(flags.get<char>() + 8);
         int* rec_ovf = reinterpret_cast<int*>(flags.get<char>() + 16);
         pglobal g{grec.get<uint64_t>(), gcap - 1, flags.get<int>(), flags.get<int>() + 1};
-        if (n > 0) {
+        bool done_units = false;
+        if (n > 0 && !gfur && !getenv("GX_PART_OLD_AGG")) {
+            // Rows were moved with their values: aggregate with the shared
+            // hash-table kernel over the partitioned copies.
+            agg_desc pd = d;
+            for (int c = 0; c < d.n_cols; ++c) pd.col_ptr[c] = mc.out[c + 1];
+            done_units = hash_units_aggregate(mc.out[0], kw, kind, pd, units.get<part_unit>(), uoff.get<int64_t>() + P,
+                                              ceil_div(bound, (int64_t)P), R, grec.get<uint64_t>(), gcap,
+                                              flags.get<int>(), orec.get<uint64_t>(), ocount, rec_cap, rec_ovf, s);
+        }
+        if (n > 0 && !done_units) {
             size_t smem = (size_t)S * per_slot;
             int per_sm = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / std::max<size_t>(smem, 1)));
             int grid = dev().sm_count * per_sm;

@@ -142,6 +142,28 @@ __global__ void __launch_bounds__(SEG_NT) k_seg_reduce(const void* __restrict__ 
         for (int a = 0; a < d.n_acc; ++a)
             acc[a] = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], acc[a], dev_::pick(v, d.acc_col[a]));
     }
+    // Tail runs: the lanes of a warp cover consecutive rows, so lanes whose
+    // open run is the same group are adjacent.  A segmented inclusive scan
+    // over the lanes folds each such stretch into its last lane, which
+    // flushes once (long runs would otherwise flush once per thread).
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const long long g = open ? (long long)cur_gid : -2 - (long long)(blockIdx.x * (int64_t)SEG_NT + threadIdx.x);
+    const long long g_next = __shfl_down_sync(FULL, g, 1);
+    const bool shares_next = lane < 31 && g_next == g;
+    if (__ballot_sync(FULL, shares_next) != 0) {
+        for (int off = 1; off < 32; off <<= 1) {
+            const long long g_up = __shfl_up_sync(FULL, g, off);
+            const unsigned long long c_up = __shfl_up_sync(FULL, cnt, off);
+            const bool take = lane >= off && g_up == g;
+            for (int a = 0; a < d.n_acc; ++a) {
+                const uint64_t a_up = __shfl_up_sync(FULL, (unsigned long long)acc[a], off);
+                if (take) acc[a] = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], acc[a], a_up);
+            }
+            if (take) cnt += c_up;
+        }
+        if (shares_next) return;  // a later lane holds the combined run
+    }
     flush();
 }
 

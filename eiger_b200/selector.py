@@ -101,68 +101,83 @@ def heuristic_algo(key) -> int:
     return gx.HASH if est <= thr else gx.PARTITION
 
 
-def _pack(instances, feats, times, ftimes, heur) -> dict:
-    return {"features": np.array(feats, np.float32).reshape(-1, F), "times": np.array(times, np.float64).reshape(-1, NV),
+def _pack(instances, index, feats, times, ftimes, heur) -> dict:
+    return {"index": np.array(index, np.int64),
+            "features": np.array(feats, np.float32).reshape(-1, F), "times": np.array(times, np.float64).reshape(-1, NV),
             "fanout_times": np.array(ftimes, np.float64).reshape(-1, len(FANOUTS)),
-            "heuristic": np.array(heur, np.int32), "instances": json.dumps(instances[:len(feats)])}
+            "heuristic": np.array(heur, np.int32), "instances": json.dumps([instances[i] for i in index])}
 
 
-def collect(instances: list[dict], fanout_every: int = 4, log=None, out: str | None = None,
-            save_every: int = 128) -> dict:
-    """Features and plain-engine timings (ms) of every variant per instance.
-    With `out`, the rows collected so far are saved every `save_every`
-    instances, and a run resumes from an existing file."""
+def collect(instances: list[dict], start: int = 0, count: int | None = None, fanout_every: int = 4, log=None,
+            out: str | None = None, save_every: int = 1) -> dict:
+    """Features and plain-engine timings (ms) of every variant for instances
+    [start, start + count).  With `out`, the rows collected so far are saved
+    every `save_every` instances and the index being measured is written to
+    `out`.progress, so a run cut short keeps its data and shows where it
+    stopped."""
     import torch
     gx = _gx()
     log = log or (lambda m: print(m, flush=True))
     reqs = [(0, gx.SUM), (0, gx.COUNT_ALL)]
-    feats, times, ftimes, heur = [], [], [], []
-    if out and Path(out).exists():
-        d = np.load(out)
-        feats, times = list(d["features"]), list(d["times"])
-        ftimes, heur = list(d["fanout_times"]), list(d["heuristic"])
-        log(f"resuming after {len(feats)} instances")
+    stop = len(instances) if count is None else min(len(instances), start + count)
+    index, feats, times, ftimes, heur = [], [], [], [], []
     phase = {"make": 0.0, "features": 0.0, "variants": 0.0, "fanouts": 0.0, "heuristic": 0.0}
 
     def clock(name, t0):
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         phase[name] += t1 - t0
+        if out:
+            Path(str(out) + ".progress").write_text(f"{idx} after {name}\n")
         return t1
 
-    for idx, inst in enumerate(instances):
-        if idx < len(feats):
-            continue
+    for idx in range(start, stop):
+        inst = instances[idx]
+        if out:
+            Path(str(out) + ".progress").write_text(f"{idx} start\n")
         t0 = time.perf_counter()
         k, v, cdf = make_instance(inst)
         t0 = clock("make", t0)
-        feats.append(features(k))
+        f = features(k)
         t0 = clock("features", t0)
         row = []
         for algo in (gx.HASH, gx.SORT, gx.PARTITION):
+            if out:
+                Path(str(out) + ".progress").write_text(f"{idx} variant {algo}\n")
             row.append(time_call(lambda: gx.groupby([k], [v], reqs, gx.make_hint(algo))))
-        times.append(row)
         t0 = clock("variants", t0)
         fr = [np.nan] * len(FANOUTS)
         if idx % fanout_every == 0:
             for j, bits in enumerate(FANOUTS):
+                if out:
+                    Path(str(out) + ".progress").write_text(f"{idx} fanout {bits}\n")
                 fr[j] = time_call(lambda: gx.groupby([k], [v], reqs, gx.make_hint(gx.PARTITION, radix_bits=bits)))
-        ftimes.append(fr)
         t0 = clock("fanouts", t0)
-        heur.append(heuristic_algo(k))
+        h = heuristic_algo(k)
         clock("heuristic", t0)
         del k, v, cdf
-        if (idx + 1) % 16 == 0:
+        index.append(idx), feats.append(f), times.append(row), ftimes.append(fr), heur.append(h)
+        if len(index) % 16 == 0:
             log(f"{idx + 1} at {time.strftime('%H:%M:%S')}: " + " ".join(f"{n}={s:.1f}s" for n, s in phase.items()))
-        if (idx + 1) % save_every == 0:
-            torch.cuda.empty_cache()
-            log(f"collected {idx + 1}/{len(instances)} at {time.strftime('%H:%M:%S')}")
-            if out:
-                np.savez(out, **_pack(instances, feats, times, ftimes, heur))
-    data = _pack(instances, feats, times, ftimes, heur)
+        if out and len(index) % save_every == 0:
+            np.savez(out, **_pack(instances, index, feats, times, ftimes, heur))
+    data = _pack(instances, index, feats, times, ftimes, heur)
     if out:
         np.savez(out, **data)
     return data
+
+
+def merge(paths: list[str]) -> dict:
+    """Concatenate collected chunks in instance order (duplicates dropped)."""
+    parts = [np.load(p) for p in paths]
+    index = np.concatenate([d["index"] for d in parts])
+    order = np.argsort(index, kind="stable")
+    keep = order[np.concatenate([[True], np.diff(index[order]) != 0])] if len(order) else order
+    insts = sum((json.loads(str(d["instances"])) for d in parts), [])
+    out = {"index": index[keep], "instances": json.dumps([insts[i] for i in keep])}
+    for key in ("features", "times", "fanout_times", "heuristic"):
+        out[key] = np.concatenate([d[key] for d in parts])[keep]
+    return out
 
 
 def targets_from(times: np.ndarray, ftimes: np.ndarray):
@@ -256,6 +271,11 @@ def main() -> None:
     c.add_argument("--instances", type=int, default=4096)
     c.add_argument("--seed", type=int, default=7)
     c.add_argument("--out", required=True)
+    c.add_argument("--start", type=int, default=0)
+    c.add_argument("--count", type=int, default=None)
+    mg = sub.add_parser("merge")
+    mg.add_argument("chunks", nargs="+")
+    mg.add_argument("--out", required=True)
     t = sub.add_parser("train")
     t.add_argument("timings")
     t.add_argument("--holdout", type=int, default=1024)
@@ -265,7 +285,10 @@ def main() -> None:
     t.add_argument("--heldout-out", default=None, help="save the held-out features / timings (for tests)")
     a = ap.parse_args()
     if a.cmd == "collect":
-        collect(draw_instances(a.instances, a.seed), out=a.out)
+        collect(draw_instances(a.instances, a.seed), start=a.start, count=a.count, out=a.out)
+        return
+    if a.cmd == "merge":
+        np.savez(a.out, **merge(a.chunks))
         return
     d = np.load(a.timings)
     x, times, ft = d["features"], d["times"], d["fanout_times"]
