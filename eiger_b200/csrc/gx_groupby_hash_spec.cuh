@@ -27,22 +27,7 @@ __device__ __forceinline__ void upd(uint64_t* p, uint64_t v) {
     } else if constexpr (OP == OP_SUM) {
         atomicAdd(reinterpret_cast<double*>(p), __longlong_as_double((long long)v));
     } else if constexpr (OP == OP_MIN || OP == OP_MAX) {
-        // Decide on the high 32 bits of the order-preserving image first (one
-        // 4-byte shared load instead of 8): they settle all but ties, which
-        // fall back to the full 64-bit comparison.
-        if constexpr (KIND == VK_F) {
-            if (__longlong_as_double((long long)v) != __longlong_as_double((long long)v)) return;  // NaN
-        }
-        auto ord_hi = [](uint32_t hi) -> uint32_t {
-            if constexpr (KIND == VK_I) return hi ^ 0x80000000u;
-            else if constexpr (KIND == VK_U) return hi;
-            else return (hi & 0x80000000u) ? ~hi : (hi ^ 0x80000000u);
-        };
-        const uint32_t vh = ord_hi((uint32_t)(v >> 32));
-        const uint32_t ch = ord_hi(reinterpret_cast<volatile uint32_t*>(p)[1]);
-        if (OP == OP_MIN ? vh > ch : vh < ch) return;
-        if (vh == ch && !dev_::improves(OP, KIND, v, *reinterpret_cast<volatile uint64_t*>(p))) return;
-        dev_::acc_atomic(p, OP, KIND, v);
+        if (dev_::improves(OP, KIND, v, *reinterpret_cast<volatile uint64_t*>(p))) dev_::acc_atomic(p, OP, KIND, v);
     } else {
         *reinterpret_cast<volatile unsigned long long*>(p) = v;
     }

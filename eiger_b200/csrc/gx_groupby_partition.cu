@@ -133,6 +133,13 @@ __global__ void __launch_bounds__(PS_NT) k_part_scatter(const void* __restrict__
             sdig[pos[k]] = (unsigned short)dig[k];
         }
     }
+    __syncthreads();
+    int64_t orow[PS_IPT];  // output row of each staged position this thread writes
+#pragma unroll
+    for (int m = 0; m < PS_IPT; ++m) {
+        const int j = threadIdx.x + m * PS_NT;
+        orow[m] = j < tile_n ? gbase[sdig[j]] + j : 0;
+    }
     for (int c = 0; c < mc.n; ++c) {
         __syncthreads();
         const int w = mc.width[c];
@@ -149,10 +156,12 @@ __global__ void __launch_bounds__(PS_NT) k_part_scatter(const void* __restrict__
             }
         }
         __syncthreads();
-        for (int j = threadIdx.x; j < tile_n; j += PS_NT) {
-            int64_t o = gbase[sdig[j]] + j;
-            if (w == 8) static_cast<unsigned long long*>(mc.out[c])[o] = stage[j];
-            else static_cast<unsigned*>(mc.out[c])[o] = (unsigned)stage[j];
+#pragma unroll
+        for (int m = 0; m < PS_IPT; ++m) {
+            const int j = threadIdx.x + m * PS_NT;
+            if (j >= tile_n) break;
+            if (w == 8) static_cast<unsigned long long*>(mc.out[c])[orow[m]] = stage[j];
+            else static_cast<unsigned*>(mc.out[c])[orow[m]] = (unsigned)stage[j];
         }
     }
 }
@@ -161,7 +170,7 @@ __global__ void __launch_bounds__(PS_NT) k_part_scatter(const void* __restrict__
 // registers up front, so all of a tile's global loads are in flight together
 // (the general kernel loads one column per staging round).
 template <int KW, int NC>
-__global__ void __launch_bounds__(PS_NT) k_part_scatter_r(const void* __restrict__ keys, int64_t n, int kind,
+__global__ void __launch_bounds__(PS_NT, 2) k_part_scatter_r(const void* __restrict__ keys, int64_t n, int kind,
                                                            int shift, int dbits, int64_t ntiles,
                                                            const int64_t* __restrict__ offsets, move_cols mc) {
     __shared__ unsigned whist[PS_WARPS * PS_BINS];
@@ -244,6 +253,15 @@ __global__ void __launch_bounds__(PS_NT) k_part_scatter_r(const void* __restrict
             sdig[pos[k]] = (unsigned short)dig[k];
         }
     }
+    // Output row of each staged position this thread writes, computed once
+    // for all columns.
+    __syncthreads();
+    int64_t orow[PS_IPT];
+#pragma unroll
+    for (int m = 0; m < PS_IPT; ++m) {
+        const int j = threadIdx.x + m * PS_NT;
+        orow[m] = j < tile_n ? gbase[sdig[j]] + j : 0;
+    }
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         __syncthreads();
@@ -254,12 +272,21 @@ __global__ void __launch_bounds__(PS_NT) k_part_scatter_r(const void* __restrict
         }
         __syncthreads();
         const int w = mc.width[c];
-        for (int j = threadIdx.x; j < tile_n; j += PS_NT) {
-            const int64_t o = gbase[sdig[j]] + j;
-            if (w == 8) static_cast<unsigned long long*>(mc.out[c])[o] = stage[j];
-            else static_cast<unsigned*>(mc.out[c])[o] = (unsigned)stage[j];
+#pragma unroll
+        for (int m = 0; m < PS_IPT; ++m) {
+            const int j = threadIdx.x + m * PS_NT;
+            if (j >= tile_n) break;
+            if (w == 8) static_cast<unsigned long long*>(mc.out[c])[orow[m]] = stage[j];
+            else static_cast<unsigned*>(mc.out[c])[orow[m]] = (unsigned)stage[j];
         }
     }
+}
+
+__global__ void k_starts_from_offsets(const int64_t* __restrict__ offs, int64_t ntiles, int P, int64_t n,
+                                      int64_t* __restrict__ ps) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < P) ps[p] = offs[(int64_t)p * ntiles];
+    else if (p == P) ps[P] = n;
 }
 
 // Work units: partition p split into ceil(size/T) units.
@@ -569,7 +596,15 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     // Partition starts: the keys are now grouped by partition id, so
     // part_start[p] is the first row whose id is >= p.
     dbuf pstart((size_t)(P + 1) * 8, s);
-    partition_starts(mc.out[0], kw, n, kind, R, pstart.get<int64_t>(), s);
+    if (passes == 1 && n > 0) {
+        // One pass: the scanned digit counts already hold each partition's
+        // start (bin p's offset in the first tile).
+        k_starts_from_offsets<<<(unsigned)ceil_div(P + 1, 256), 256, 0, s>>>(offs.get<int64_t>(), ntiles, P, n,
+                                                                            pstart.get<int64_t>());
+        GX_LAUNCHED();
+    } else {
+        partition_starts(mc.out[0], kw, n, kind, R, pstart.get<int64_t>(), s);
+    }
 
     // Work units.
     // Split threshold: partitions above twice the mean size are split (Zipf
