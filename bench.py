@@ -434,7 +434,7 @@ def run_reference(args) -> None:
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
-            "config": {"workload": f"hash group-by, {args.rows} rows, int32 keys uniform over {G} scattered "
+            "config": {"workload": f"group-by (oracle hash aggregation), {args.rows} rows, int32 keys uniform over {G} scattered "
                                    "values, int64 + float64 values, SUM/COUNT/MIN/MAX on both",
                        "rows": args.rows, "groups": G, "sample_rows": rows},
             "cpu_baseline": {"value": value, "unit": "Mrows/s", "cores": O.num_threads(), "kind": "port",

@@ -403,7 +403,8 @@ __device__ __forceinline__ int64_t lookback(unsigned long long* tstate, int64_t 
     return excl;
 }
 
-template <int KW>
+// ROWIDS: the output is just the (build row, probe row) pair (int64 each).
+template <int KW, bool ROWIDS>
 __global__ void __launch_bounds__(JP_NT) k_dense_probe1(const void* __restrict__ pkeys, int64_t np, int kind,
                                                          uint64_t lo, uint64_t hi,
                                                          const uint32_t* __restrict__ slot_row,
@@ -448,16 +449,23 @@ __global__ void __launch_bounds__(JP_NT) k_dense_probe1(const void* __restrict__
             int64_t pos = wbase + __popc(bal & lt);
             int64_t i = row0 + k * 32;
             if (pos < np) {  // capacity bound (a unique-key probe never exceeds it)
-                if (o.key) st_w(o.key, o.key_width, pos, ld_w(pkeys, o.key_width, i));
-                for (int cc = 0; cc < o.n_pay; ++cc) {
-                    uint64_t v;
-                    switch (o.src[cc]) {
-                        case 1: v = ld_w(o.col[cc], o.width[cc], (int64_t)m[k]); break;
-                        case 2: v = ld_w(o.col[cc], o.width[cc], i); break;
-                        case 3: v = (uint64_t)m[k]; break;
-                        default: v = (uint64_t)i; break;
+                if constexpr (ROWIDS) {
+                    const int64_t b = (int64_t)m[k];
+                    const bool build_first = o.src[0] == 3;
+                    static_cast<int64_t*>(o.out[0])[pos] = build_first ? b : i;
+                    static_cast<int64_t*>(o.out[1])[pos] = build_first ? i : b;
+                } else {
+                    if (o.key) st_w(o.key, o.key_width, pos, ld_w(pkeys, o.key_width, i));
+                    for (int cc = 0; cc < o.n_pay; ++cc) {
+                        uint64_t v;
+                        switch (o.src[cc]) {
+                            case 1: v = ld_w(o.col[cc], o.width[cc], (int64_t)m[k]); break;
+                            case 2: v = ld_w(o.col[cc], o.width[cc], i); break;
+                            case 3: v = (uint64_t)m[k]; break;
+                            default: v = (uint64_t)i; break;
+                        }
+                        st_w(o.out[cc], o.width[cc], pos, v);
                     }
-                    st_w(o.out[cc], o.width[cc], pos, v);
                 }
             }
         }
@@ -539,14 +547,16 @@ static bool dense_join(const join_inputs& in, const gx_join_hint& hint, bool row
         int* err = reinterpret_cast<int*>(scal.get<char>() + 8);
         {
             GX_PROF("join_probe_write", s);
-            if (kw == 4)
-                k_dense_probe1<4><<<(unsigned)ntiles, JP_NT, 0, s>>>(pkey.data, np, kind, lo, hi, slot_row.get<uint32_t>(),
-                                                                     tstate.get<unsigned long long>(), ticket, ntiles,
-                                                                     total_out, err, o);
-            else
-                k_dense_probe1<8><<<(unsigned)ntiles, JP_NT, 0, s>>>(pkey.data, np, kind, lo, hi, slot_row.get<uint32_t>(),
-                                                                     tstate.get<unsigned long long>(), ticket, ntiles,
-                                                                     total_out, err, o);
+#define GX_PROBE1(KW_, RID_)                                                                            \
+    k_dense_probe1<KW_, RID_><<<(unsigned)ntiles, JP_NT, 0, s>>>(pkey.data, np, kind, lo, hi,              \
+                                                                 slot_row.get<uint32_t>(),                \
+                                                                 tstate.get<unsigned long long>(), ticket, \
+                                                                 ntiles, total_out, err, o)
+            if (kw == 4 && rowids_only) GX_PROBE1(4, true);
+            else if (kw == 4) GX_PROBE1(4, false);
+            else if (rowids_only) GX_PROBE1(8, true);
+            else GX_PROBE1(8, false);
+#undef GX_PROBE1
             GX_LAUNCHED();
         }
         int64_t hs[2];
