@@ -283,7 +283,16 @@ def run_gx(args) -> None:
         # Table form [key, build payload, probe payload] with int64 payloads.
         join["table_form"] = measure(lambda: gx.inner_eq_join([bk, brow], [pk, prow], jh),
                                      lambda m: (nb + npr) * 12 + m * 20)
-        del bk, brow, pk, prow
+        # Second probe set: Zipf s = 1.0 over the build keys (rank r -> the
+        # r-th build key, so hot probe keys are spread over the key space).
+        cdf = torch.from_numpy(gx.zipf_cdf(nb, 1.0)).cuda()
+        zr = torch.empty(npr, dtype=torch.int32, device="cuda")
+        gx.generate_keys(zr, gx.gen_spec(seed=41 + rank, dist=gx.DIST_ZIPF, groups=nb, zipf_s=1.0,
+                                         zipf_cdf=cdf.data_ptr()))
+        zpk = bk[zr.long()]
+        del zr, cdf
+        join["zipf_1.0"] = measure(lambda: gx.inner_eq_join_rowids(bk, zpk, jh), lambda m: (nb + npr) * 4 + m * 16)
+        del bk, brow, pk, prow, zpk
 
     # ----------------------------------------------------------- batched
     batched = None
@@ -397,6 +406,23 @@ def run_sweep(args) -> None:
                 torch.cuda.empty_cache()
 
 
+def run_join_only(args) -> None:
+    """The C3 rowid join alone (for profiling captures): 2^24 unique build
+    keys x --join-rows probe keys (10% absent); prints one JSON line."""
+    import torch
+    import eiger_b200 as gx
+    torch.cuda.set_device(0)
+    nb, npr = 1 << 24, args.join_rows
+    bk = torch.empty(nb, dtype=torch.int32, device="cuda")
+    gx.generate_permutation(bk, 42)
+    pk = torch.empty(npr, dtype=torch.int32, device="cuda")
+    gx.generate_keys(pk, gx.gen_spec(seed=39, groups=nb, miss_frac=0.1))
+    jh = gx.make_join_hint(gx.JOIN_SORT, gx.MAT_GFUR, unique_left=1)
+    ms = time_steps(torch, lambda: gx.inner_eq_join_rowids(bk, pk, jh), args.steps, args.warmup) / args.steps
+    print(json.dumps({"workload": f"rowid join, 2^24 unique int32 build keys x {npr} probe keys (10% absent)",
+                      "ms_per_step": ms, "value": (nb + npr) / (ms * 1e-3) / 1e6, "unit": "Mrows/s"}), flush=True)
+
+
 def cpu_groupby_baseline(rows: int, groups: int) -> dict:
     """The oracle (CPU restatement, all host threads) on a bounded sample."""
     import oracle as O
@@ -456,6 +482,7 @@ def main() -> None:
                     help="group-by variant (auto: the engine's plain selection rule)")
     ap.add_argument("--join-rows", type=int, default=1 << 28)
     ap.add_argument("--no-join", action="store_true")
+    ap.add_argument("--join-only", action="store_true", help="only the rowid join (profiling captures)")
     ap.add_argument("--batch-instances", type=int, default=512, help="batched pipeline instances (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=1 << 24)
@@ -472,6 +499,9 @@ def main() -> None:
         args.warmup = 3
     if args.sweep:
         run_sweep(args)
+        return
+    if args.join_only:
+        run_join_only(args)
         return
     if args.impl == "reference":
         run_reference(args)

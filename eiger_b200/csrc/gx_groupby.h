@@ -8,6 +8,9 @@ namespace gx {
 // ----- hash group-by (gx_groupby_hash.cu) -----
 void init_records(uint64_t* recs, int64_t nrec, const agg_desc& d, uint64_t empty, cudaStream_t s);
 int hash_smem_slots(const agg_desc& d, int key_width, int64_t groups_bound, int* replicas);
+// Sample sketch of a key column (gx_selector.cu): f[6..13] are the shares of
+// the 8 most frequent keys in a 2^14-row strided sample.
+void selector_features(const col& key, float* f, cudaStream_t s);
 // A work unit of radix-partitioned rows: rows [begin, end) of one partition;
 // split = the partition is spread over several units.
 struct part_unit {
