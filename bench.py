@@ -1,8 +1,9 @@
 #!/usr/bin/env python
 """Benchmark of the relational operator core on B200.
 
-Default workload (one "step"): group-by over 2^28 rows (variant chosen by the
-engine's plain AUTO rule unless --algo names one) — int32 keys
+Default workload (one "step"): group-by over 2^28 rows (AUTO: variant chosen by
+the learned selector with the committed weights; --selector plain for the
+reference's NDV rule, --algo to force one) — int32 keys
 (scattered, uniform over --groups distinct values), an int64 column uniform
 in [0, 2^31) and a float64 column uniform in [0, 1), SUM / COUNT / MIN / MAX
 on both value columns (the group-by sweep configuration, one point of it).
@@ -177,9 +178,15 @@ def run_gx(args) -> None:
     reqs = groupby_reqs(gx)
     hint_algo = {"auto": gx.AUTO_ALGO, "hash": gx.HASH, "sort": gx.SORT, "partition": gx.PARTITION}[args.algo]
     chosen = {}
+    # AUTO with the learned selector (committed weights) unless --selector plain.
+    learned = False
+    if args.algo == "auto" and args.selector == "learned":
+        from eiger_b200 import selector as sel_mod
+        learned = sel_mod.install()
+    sel = gx.SELECT_LEARNED if learned else gx.SELECT_HEURISTIC
 
     def step():
-        h = gx.make_hint(hint_algo, G)
+        h = gx.make_hint(hint_algo, G, selector=sel)
         t = gx.groupby([k], [iv, fv], reqs, h)
         chosen["algo"], chosen["radix_bits"] = h.groupby_algo, h.radix_bits
         return t
@@ -233,7 +240,7 @@ def run_gx(args) -> None:
         dk = hk.to("cuda", non_blocking=True)
         div = hiv.to("cuda", non_blocking=True)
         dfv = hfv.to("cuda", non_blocking=True)
-        t = gx.groupby([dk], [div, dfv], reqs, gx.make_hint(hint_algo, G))
+        t = gx.groupby([dk], [div, dfv], reqs, gx.make_hint(hint_algo, G, selector=sel))
         cols = t.numpy_columns()  # device -> host read of the result
         return cols
 
@@ -340,6 +347,7 @@ def run_gx(args) -> None:
                                    "SUM/COUNT/MIN/MAX on both",
                        "rows": rows, "groups": G, "groups_found": ngroups, "algo": args.algo,
                        "variant_run": algo_name, "radix_bits": chosen.get("radix_bits"),
+                       "selector": "learned" if learned else ("plain" if args.algo == "auto" else "forced"),
                        "l2": "inputs (5.4 GB) larger than L2; no flush"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk.summary(), "join": join, "batched": batched,
@@ -483,6 +491,8 @@ def main() -> None:
     ap.add_argument("--join-rows", type=int, default=1 << 28)
     ap.add_argument("--no-join", action="store_true")
     ap.add_argument("--join-only", action="store_true", help="only the rowid join (profiling captures)")
+    ap.add_argument("--selector", choices=["learned", "plain"], default="learned",
+                    help="AUTO's chooser: the learned FP16 MLP (committed weights) or the plain NDV rule")
     ap.add_argument("--batch-instances", type=int, default=512, help="batched pipeline instances (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=1 << 24)
