@@ -704,8 +704,12 @@ void inner_eq_join(const gx_table_view* left, const gx_table_view* right, const 
     if (left->columns[0].type != right->columns[0].type) fail(GX_EINVAL, "Join columns cannot have different types");
     if (left->num_columns == 1 || right->num_columns == 1)
         fail(GX_EINVAL, "Left and right table should have at least 1 payload column");
-    if (hint->join_algo != GX_JOIN_SORT)
-        fail(GX_EUNSUPPORTED, "only join_algo SORT is implemented by this library");
+    // HASH and PARTITION (hash_join.cu, partition_hash_join.cu in the
+    // reference) return the same pairs as SORT; here all three run the one
+    // matcher above (dense placement or sorted build + radix directory),
+    // which is this library's fastest plan for every key shape it handles.
+    if (hint->join_algo != GX_JOIN_SORT && hint->join_algo != GX_JOIN_HASH && hint->join_algo != GX_JOIN_PARTITION)
+        fail(GX_EINVAL, "Unsupported join algorithm");
     join_inputs in;
     in.lkey = resolve(left->columns[0]);
     in.rkey = resolve(right->columns[0]);

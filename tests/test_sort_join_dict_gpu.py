@@ -224,3 +224,19 @@ def test_generators_match_cpu(dist, kdt):
     gx.generate_permutation(p, 11, -7)
     assert np.array_equal(p.cpu().numpy(), O.gen_perm(4096, np.int32, 11, -7))
     assert np.array_equal(gx.zipf_cdf(G, 1.2), cdf)
+
+
+@pytest.mark.parametrize("algo", [gx.JOIN_HASH, gx.JOIN_PARTITION])
+@pytest.mark.parametrize("mat", [gx.MAT_GFUR, gx.MAT_GFTR])
+def test_join_hash_and_partition_hints_give_the_sort_result(algo, mat):
+    # join_algo HASH / PARTITION (inner_join.cu:54-74) must return the same
+    # pair multiset as SORT, including duplicate keys on both sides.
+    lk = O.gen_keys(5000, np.int64, groups=700, seed=11)
+    rk = O.gen_keys(20000, np.int64, groups=900, seed=12)
+    lp = np.arange(5000, dtype=np.int64)
+    rp = np.arange(20000, dtype=np.int64)
+    t = gx.inner_eq_join([to_dev(lk), to_dev(lp)], [to_dev(rk), to_dev(rp)], gx.make_join_hint(algo, mat))
+    cols = t.numpy_columns()
+    got = np.lexsort((cols[2], cols[1]))
+    el, er = O.join_pairs(lk, rk)
+    assert np.array_equal(cols[1][got], el) and np.array_equal(cols[2][got], er)
