@@ -317,25 +317,38 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
                     }
                 }
             }
+            // First probe of every row of the batch at once (independent
+            // shared loads); only a row whose home slot holds another key
+            // (or is empty) walks the probe sequence.
+            uint32_t h[HGB_UNROLL];
+            int slot[HGB_UNROLL];
 #pragma unroll
             for (int q = 0; q < HGB_UNROLL; ++q) {
-                const int64_t i = base + q * HGB_NT + threadIdx.x;
-                const bool valid = i < un.end;
-                uint32_t h = 0;
-                int slot = -1;
-                if (valid) {
-                    h = key_hash<KW>(kw[q]);
-                    slot = s_find_or_insert<KW>(st, kw[q], h >> shift);
+                const bool valid = base + q * HGB_NT + threadIdx.x < un.end;
+                h[q] = valid ? key_hash<KW>(kw[q]) : 0u;
+                slot[q] = -2;
+                if (valid && (kt)kw[q] != EMPTY) {
+                    const uint32_t s0 = (h[q] >> shift) & st.mask;
+                    if (((volatile kt*)st.keys)[s0] == (kt)kw[q]) slot[q] = (int)s0;
                 }
-                __syncwarp();  // regroup after the probe loop (see k_hash_groupby)
+            }
+#pragma unroll
+            for (int q = 0; q < HGB_UNROLL; ++q) {
+                const bool valid = base + q * HGB_NT + threadIdx.x < un.end;
+                if (valid && slot[q] == -2) slot[q] = s_find_or_insert<KW>(st, kw[q], h[q] >> shift);
+            }
+            __syncwarp();  // regroup after the probe loops (see k_hash_groupby)
+#pragma unroll
+            for (int q = 0; q < HGB_UNROLL; ++q) {
+                const bool valid = base + q * HGB_NT + threadIdx.x < un.end;
                 if (!valid) continue;
-                if (slot >= 0) {
-                    atomicAdd(&my_counts[slot], 1u);
-                    if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, slot, v[q]);
-                    else dev_::shared_row_update<NV>(my_acc, s_slots, slot, d, v[q]);
+                if (slot[q] >= 0) {
+                    atomicAdd(&my_counts[slot[q]], 1u);
+                    if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, slot[q], v[q]);
+                    else dev_::shared_row_update<NV>(my_acc, s_slots, slot[q], d, v[q]);
                 } else {
                     if (!s_spill) s_spill = 1;
-                    uint64_t* r = g_find_or_insert<KW>(g, d, kw[q], h);
+                    uint64_t* r = g_find_or_insert<KW>(g, d, kw[q], h[q]);
                     if (r) g_update(r, d, v[q], 1ull);
                 }
             }

@@ -39,24 +39,6 @@ __device__ __forceinline__ uint64_t ld_key(const void* p, int64_t i, int kind) {
     return canon64(__ldg(static_cast<const unsigned long long*>(p) + i), kind);
 }
 
-template <int KW>
-__global__ void __launch_bounds__(PS_NT) k_part_hist(const void* __restrict__ keys, int64_t n, int kind,
-                                                      int shift, int dbits, int64_t ntiles,
-                                                      int64_t* __restrict__ counts) {
-    __shared__ unsigned hist[PS_BINS];
-    const int bins = 1 << dbits;
-    for (int b = threadIdx.x; b < bins; b += PS_NT) hist[b] = 0;
-    __syncthreads();
-    int64_t base = blockIdx.x * (int64_t)PS_TILE;
-#pragma unroll
-    for (int k = 0; k < PS_IPT; ++k) {
-        int64_t i = base + k * PS_NT + threadIdx.x;
-        if (i < n) atomicAdd(&hist[(part_hash<KW>(ld_key<KW>(keys, i, kind)) >> shift) & (bins - 1)], 1u);
-    }
-    __syncthreads();
-    for (int b = threadIdx.x; b < bins; b += PS_NT) counts[(int64_t)b * ntiles + blockIdx.x] = hist[b];
-}
-
 struct move_cols {
     int n;
     const void* in[MAX_VCOLS + 2];
@@ -282,6 +264,304 @@ __global__ void __launch_bounds__(PS_NT, 2) k_part_scatter_r(const void* __restr
     }
 }
 
+// ---------------------------------------------------------------------------
+// Bulk-copy scatter: one persistent CTA per SM walks its tiles (blockIdx.x,
+// + gridDim.x, ...), with each tile's column slices brought into shared
+// memory by the copy engine (cp.async.bulk on an mbarrier) one tile ahead, so
+// the loads of tile t+1 overlap the ranking and writes of tile t and no
+// column value occupies a register.  A tile is ranked exactly as in
+// k_part_scatter (stable: digit, then row order), then each output position
+// j reads its source row from the shared copy and writes every column to
+// gbase[digit] + j.  Used when every loaded column starts on a 16-byte
+// boundary and two tiles of the columns fit in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int PB_NT = 1024;
+constexpr int PB_WARPS = PB_NT / 32;
+constexpr int PB_IPT = PS_TILE / PB_NT;  // 4
+constexpr uint32_t PB_WAIT_LIMIT = 1u << 22;
+
+struct pb_layout {
+    uint32_t in_off[MAX_VCOLS + 2];  // column c's slice within one stage
+    uint32_t stage_bytes;            // one tile of every loaded column
+    uint32_t whist, qsum, src, sdig, gbase, dbase, total;
+};
+
+__host__ __device__ inline pb_layout pb_make_layout(const move_cols& mc) {
+    pb_layout L{};
+    uint32_t o = 0;
+    for (int c = 0; c < mc.n; ++c) {
+        L.in_off[c] = o;
+        if (!mc.iota[c]) o += (uint32_t)PS_TILE * (uint32_t)mc.width[c];
+    }
+    L.stage_bytes = o;
+    o *= 2;
+    L.whist = o; o += PB_WARPS * PS_BINS * 2;   // u16 per-warp digit counts
+    L.qsum = o;  o += 4 * PS_BINS * 2;          // u16 sums over 8-warp quarters
+    L.src = o;   o += PS_TILE * 2;              // u16 source row of each staged position
+    L.sdig = o;  o += PS_TILE;                  // u8 digit of each staged position
+    L.gbase = o; o += PS_BINS * 8;              // int64 output base per digit
+    L.dbase = o; o += PS_BINS * 4;              // u32 first staged position per digit
+    L.total = o;
+    return L;
+}
+
+template <int KW, int NC>
+__global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __restrict__ keys, int64_t n, int kind,
+                                                                int shift, int dbits, int64_t ntiles,
+                                                                const int64_t* __restrict__ offsets, move_cols mc,
+                                                                pb_layout L, int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char pb_smem[];
+    __shared__ __align__(8) unsigned long long bars[2];
+    __shared__ unsigned wsum[PS_BINS / 32];
+    __shared__ int s_err;
+    unsigned short* whist = reinterpret_cast<unsigned short*>(pb_smem + L.whist);
+    unsigned short* qsum = reinterpret_cast<unsigned short*>(pb_smem + L.qsum);
+    unsigned short* src = reinterpret_cast<unsigned short*>(pb_smem + L.src);
+    unsigned char* sdig = pb_smem + L.sdig;
+    int64_t* gbase = reinterpret_cast<int64_t*>(pb_smem + L.gbase);
+    unsigned* dbase = reinterpret_cast<unsigned*>(pb_smem + L.dbase);
+
+    const int bins = 1 << dbits;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const uint32_t bar0 = dev_::smem_addr(&bars[0]);
+    // Issues the copies of tile `tile` into stage `b` (thread 0 only; full
+    // tiles only — the last, partial tile is loaded with plain loads).
+    auto issue = [&](int64_t tile, int b) {
+        const uint32_t bar = bar0 + 8u * (uint32_t)b;
+        dev_::mbar_arrive_expect_tx(bar, L.stage_bytes);
+        const uint32_t base = dev_::smem_addr(pb_smem) + (uint32_t)b * L.stage_bytes;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            if (mc.iota[c]) continue;
+            const uint32_t bytes = (uint32_t)PS_TILE * (uint32_t)mc.width[c];
+            dev_::bulk_load_g2s(base + L.in_off[c],
+                                static_cast<const unsigned char*>(mc.in[c]) + tile * (int64_t)bytes, bytes, bar);
+        }
+    };
+    auto full = [&](int64_t tile) { return (tile + 1) * (int64_t)PS_TILE <= n; };
+    if (t == 0) {
+        dev_::mbar_init(bar0, 1);
+        dev_::mbar_init(bar0 + 8, 1);
+        dev_::mbar_init_fence();
+        s_err = 0;
+    }
+    __syncthreads();
+    // A copy into stage b was issued and not yet waited for: tracked by
+    // thread 0, the only issuer.
+    // Bit b of `pending` / `phase`: stage b's copy state and barrier parity.
+    uint32_t pending = 0, phase = 0;
+    if (t == 0) {
+        for (int b = 0; b < 2; ++b) {
+            const int64_t tile = blockIdx.x + (int64_t)b * gridDim.x;
+            if (tile < ntiles && full(tile)) { issue(tile, b); pending |= 1u << b; }
+        }
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    int it = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int b = it & 1;
+        unsigned char* stage = pb_smem + (size_t)b * L.stage_bytes;
+        const int64_t tile_base = tile * (int64_t)PS_TILE;
+        const int tile_n = (int)min((int64_t)PS_TILE, n - tile_base);
+        // Digit offsets of this tile (read early; used after the scan).
+        const int64_t my_off = t < bins ? offsets[(int64_t)t * ntiles + tile] : 0;
+        if (full(tile)) {
+            if (dev_::mbar_wait_bounded(bar0 + 8u * (uint32_t)b, (phase >> b) & 1u, PB_WAIT_LIMIT)) {
+                phase ^= 1u << b;
+                pending &= ~(1u << b);
+            } else {
+                s_err = 1;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (mc.iota[c]) continue;
+                if (mc.width[c] == 8) {
+                    auto* d = reinterpret_cast<unsigned long long*>(stage + L.in_off[c]);
+                    for (int i = t; i < tile_n; i += PB_NT)
+                        d[i] = __ldg(static_cast<const unsigned long long*>(mc.in[c]) + tile_base + i);
+                } else {
+                    auto* d = reinterpret_cast<unsigned*>(stage + L.in_off[c]);
+                    for (int i = t; i < tile_n; i += PB_NT)
+                        d[i] = __ldg(static_cast<const unsigned*>(mc.in[c]) + tile_base + i);
+                }
+            }
+            __syncthreads();
+        }
+        // Rank: per-warp stable digit counts (rows warp*128 + k*32 + lane).
+        for (int i = lane; i < PS_BINS; i += 32) whist[warp * PS_BINS + i] = 0;
+        __syncwarp();
+        unsigned dig[PB_IPT], rank[PB_IPT];
+#pragma unroll
+        for (int k = 0; k < PB_IPT; ++k) {
+            const int local = warp * 32 * PB_IPT + k * 32 + lane;
+            const bool valid = local < tile_n;
+            uint64_t kb = 0;
+            if (valid) {
+                if (KW == 4) kb = canon32(reinterpret_cast<const unsigned*>(stage + L.in_off[0])[local], kind);
+                else kb = canon64(reinterpret_cast<const unsigned long long*>(stage + L.in_off[0])[local], kind);
+            }
+            const unsigned d = valid ? (part_hash<KW>(kb) >> shift) & (bins - 1) : 0xFFFFu;
+            dig[k] = d;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const unsigned r = __popc(peers & lt);
+            const unsigned prior = valid ? whist[warp * PS_BINS + d] : 0;
+            rank[k] = prior + r;
+            __syncwarp();
+            if (valid && r == 0) whist[warp * PS_BINS + d] = (unsigned short)(prior + __popc(peers));
+            __syncwarp();
+        }
+        __syncthreads();
+        if (s_err) break;
+        // Cross-warp exclusive prefix per digit: thread (q, bin) sums warps 8q..8q+7.
+        const int bq = t & (PS_BINS - 1), q = t >> 8;
+        unsigned v[8], s = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) { v[j] = whist[(q * 8 + j) * PS_BINS + bq]; s += v[j]; }
+        qsum[q * PS_BINS + bq] = (unsigned short)s;
+        __syncthreads();
+        unsigned run = 0, tot = 0, incl = 0;
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+            const unsigned x = qsum[qq * PS_BINS + bq];
+            if (qq < q) run += x;
+            tot += x;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) { whist[(q * 8 + j) * PS_BINS + bq] = (unsigned short)run; run += v[j]; }
+        if (t < PS_BINS) {
+            incl = dev_::warp_inclusive_sum(tot);
+            if (lane == 31) wsum[warp] = incl;
+        }
+        __syncthreads();
+        if (t < PS_BINS) {
+            unsigned ex = incl - tot;
+            for (int w = 0; w < warp; ++w) ex += wsum[w];
+            dbase[t] = ex;
+            gbase[t] = my_off - (int64_t)ex;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PB_IPT; ++k) {
+            const int local = warp * 32 * PB_IPT + k * 32 + lane;
+            if (local < tile_n) {
+                const unsigned pos = dbase[dig[k]] + whist[warp * PS_BINS + dig[k]] + rank[k];
+                src[pos] = (unsigned short)local;
+                sdig[pos] = (unsigned char)dig[k];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < PB_IPT; ++m) {
+            const int j = t + m * PB_NT;
+            if (j >= tile_n) break;
+            const int64_t orow = gbase[sdig[j]] + j;
+            const int sr = src[j];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (mc.iota[c]) {
+                    static_cast<unsigned long long*>(mc.out[c])[orow] = (unsigned long long)(tile_base + sr);
+                } else if (mc.width[c] == 8) {
+                    static_cast<unsigned long long*>(mc.out[c])[orow] =
+                        reinterpret_cast<const unsigned long long*>(stage + L.in_off[c])[sr];
+                } else {
+                    static_cast<unsigned*>(mc.out[c])[orow] = reinterpret_cast<const unsigned*>(stage + L.in_off[c])[sr];
+                }
+            }
+        }
+        __syncthreads();
+        // Stage b is free again: prefetch the tile after next into it (the
+        // proxy fence orders this CTA's reads of the stage before the copy).
+        if (t == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            const int64_t nt = tile + 2 * (int64_t)gridDim.x;
+            if (nt < ntiles && full(nt)) { issue(nt, b); pending |= 1u << b; }
+        }
+    }
+    if (s_err) {
+        // A copy never completed: report it and wait (bounded) for the copies
+        // still in flight into this CTA's shared memory before leaving.
+        if (t == 0) {
+            atomicExch(err, 1);
+            for (int b = 0; b < 2; ++b)
+                if ((pending >> b) & 1u) dev_::mbar_wait_bounded(bar0 + 8u * (uint32_t)b, (phase >> b) & 1u, PB_WAIT_LIMIT);
+        }
+        __syncthreads();
+    }
+}
+
+// Per-tile digit counts with one warp per 4096-row tile: a warp-private
+// shared histogram, no block-wide barriers, 16 loads in flight per thread.
+constexpr int PH_NT = 256;
+constexpr int PH_WARPS = PH_NT / 32;
+template <int KW>
+__global__ void __launch_bounds__(PH_NT) k_part_hist(const void* __restrict__ keys, int64_t n, int kind, int shift,
+                                                       int dbits, int64_t ntiles, int64_t* __restrict__ counts) {
+    __shared__ unsigned hist[PH_WARPS][PS_BINS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned bmask = (1u << dbits) - 1u;
+    unsigned* h = hist[warp];
+    for (int i = lane; i < PS_BINS; i += 32) h[i] = 0;
+    __syncwarp();
+    const bool vec = (reinterpret_cast<uintptr_t>(keys) & 15) == 0;
+    for (int64_t tile = blockIdx.x * (int64_t)PH_WARPS + warp; tile < ntiles; tile += (int64_t)gridDim.x * PH_WARPS) {
+        const int64_t base = tile * (int64_t)PS_TILE;
+        const int tile_n = (int)min((int64_t)PS_TILE, n - base);
+        if (vec && tile_n == PS_TILE) {
+            // Full tile from a 16-byte aligned column: 16-byte loads, eight
+            // in flight per thread (32 keys of 4 bytes, or 16 of 8).
+            constexpr int KPV = 16 / KW, NVEC = PS_TILE / KPV, B = 8;
+            const uint4* kv = reinterpret_cast<const uint4*>(static_cast<const unsigned char*>(keys) + base * KW);
+            for (int j0 = 0; j0 < NVEC; j0 += 32 * B) {
+                uint4 x[B];
+#pragma unroll
+                for (int q = 0; q < B; ++q) x[q] = __ldcs(kv + j0 + q * 32 + lane);
+#pragma unroll
+                for (int q = 0; q < B; ++q) {
+                    if (KW == 4) {
+                        const unsigned w[4] = {x[q].x, x[q].y, x[q].z, x[q].w};
+#pragma unroll
+                        for (int e = 0; e < 4; ++e)
+                            atomicAdd(&h[(part_hash<4>(canon32(w[e], kind)) >> shift) & bmask], 1u);
+                    } else {
+                        const uint64_t w[2] = {((uint64_t)x[q].y << 32) | x[q].x, ((uint64_t)x[q].w << 32) | x[q].z};
+#pragma unroll
+                        for (int e = 0; e < 2; ++e)
+                            atomicAdd(&h[(part_hash<8>(canon64(w[e], kind)) >> shift) & bmask], 1u);
+                    }
+                }
+            }
+            __syncwarp();
+            for (int i = lane; i <= (int)bmask; i += 32) {
+                counts[(int64_t)i * ntiles + tile] = h[i];
+                h[i] = 0;
+            }
+            __syncwarp();
+            continue;
+        }
+        constexpr int B = 16;
+        for (int j0 = 0; j0 < PS_TILE; j0 += 32 * B) {
+            uint64_t kb[B];
+#pragma unroll
+            for (int q = 0; q < B; ++q) {
+                const int local = j0 + q * 32 + lane;
+                kb[q] = local < tile_n ? ld_key<KW>(keys, base + local, kind) : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < B; ++q) {
+                const int local = j0 + q * 32 + lane;
+                if (local < tile_n) atomicAdd(&h[(part_hash<KW>(kb[q]) >> shift) & bmask], 1u);
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i <= (int)bmask; i += 32) {
+            counts[(int64_t)i * ntiles + tile] = h[i];
+            h[i] = 0;
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void k_starts_from_offsets(const int64_t* __restrict__ offs, int64_t ntiles, int P, int64_t n,
                                       int64_t* __restrict__ ps) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -488,13 +768,45 @@ void partition_starts(const void* keys, int kw, int64_t n, int kind, int R, int6
 
 namespace {
 
+// The bulk-copy scatter applies when every loaded column is 4 or 8 bytes
+// wide and 16-byte aligned, and two tiles of them fit in shared memory.
+static bool bulk_scatter_ok(const move_cols& mc, const pb_layout& L) {
+    if (getenv("GX_PART_NO_BULK") || mc.n < 2 || mc.n > 3) return false;
+    for (int c = 0; c < mc.n; ++c) {
+        if (mc.iota[c]) continue;
+        if (mc.width[c] != 4 && mc.width[c] != 8) return false;
+        if (reinterpret_cast<uintptr_t>(mc.in[c]) % 16 != 0) return false;
+    }
+    return L.total <= (uint32_t)dev().max_smem_optin - 1024;
+}
+
 template <int KW>
 void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_cols& mc, int64_t* counts,
-               int64_t* offs, cudaStream_t s) {
+               int64_t* offs, int* err, cudaStream_t s) {
     int64_t ntiles = ceil_div(n, PS_TILE);
-    k_part_hist<KW><<<(unsigned)ntiles, PS_NT, 0, s>>>(kin, n, kind, shift, dbits, ntiles, counts);
+    const int hist_grid = (int)std::min<int64_t>(ceil_div(ntiles, PH_WARPS), (int64_t)dev().sm_count * 8);
+    k_part_hist<KW><<<hist_grid, PH_NT, 0, s>>>(kin, n, kind, shift, dbits, ntiles, counts);
     GX_LAUNCHED();
     exclusive_scan_i64(counts, offs, ((int64_t)1 << dbits) * ntiles, s);
+    const pb_layout L = pb_make_layout(mc);
+    if (bulk_scatter_ok(mc, L)) {
+        static bool battr[16] = {};
+        if (!battr[dev().device]) {
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         dev().max_smem_optin - 1024));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         dev().max_smem_optin - 1024));
+            battr[dev().device] = true;
+        }
+        const int grid = (int)std::min<int64_t>(ntiles, dev().sm_count);
+        GX_PROF("partition_scatter", s);
+        if (mc.n == 2)
+            k_part_scatter_bulk<KW, 2><<<grid, PB_NT, L.total, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc, L, err);
+        else
+            k_part_scatter_bulk<KW, 3><<<grid, PB_NT, L.total, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc, L, err);
+        GX_LAUNCHED();
+        return;
+    }
     const int dyn = PS_TILE * 10;
     static bool attr[16] = {};
     if (!attr[dev().device]) {
@@ -573,6 +885,8 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
 
     int64_t ntiles = ceil_div(std::max<int64_t>(n, 1), PS_TILE);
     dbuf counts((size_t)PS_BINS * ntiles * 8, s), offs((size_t)PS_BINS * ntiles * 8 + 8, s);
+    dbuf perr(sizeof(int), s);  // set by the bulk-copy scatter when a copy wait gave up
+    GX_CUDA(cudaMemsetAsync(perr.get(), 0, sizeof(int), s));
     int passes = (R + 7) / 8;
     // Two digit passes ping-pong between bufs_a and bufs_b.
     if (passes == 2)
@@ -588,8 +902,8 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
                 for (int c = 0; c < mc.n; ++c) { m.in[c] = bufs_b[c].get(); m.iota[c] = 0; m.out[c] = bufs_a[c].get(); }
             }
             const void* kin = m.in[0];
-            if (kw == 4) part_pass<4>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), s);
-            else part_pass<8>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), s);
+            if (kw == 4) part_pass<4>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr.get<int>(), s);
+            else part_pass<8>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr.get<int>(), s);
             shift += dbits;
         }
     }
@@ -625,6 +939,7 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     // Split units merge through the spill table, so size it for every group
     // when any partition was split; otherwise it only catches overflow.
     int64_t total_units = read_scalar(uoff.get<int64_t>() + P, s);
+    if (read_scalar(perr.get<int>(), s)) fail(GX_ETIMEOUT, "partition scatter: a bulk copy into shared memory did not complete");
     int64_t live_parts = std::min<int64_t>(P, n);
     uint64_t gcap = 1u << 16;
     // Also when partitions hold more groups than a shared table (radix bits

@@ -186,3 +186,36 @@ def test_closed_form_uniform_2_28_property():
         assert len(keys) == G
         assert np.all(s0 == n // G) and np.all(s1 == n // G)
         assert int(keys.astype(np.int64).sum()) == G * (G - 1) // 2
+
+
+@pytest.mark.parametrize("kdt,bits", [(np.int32, 8), (np.int64, 12)])
+@pytest.mark.parametrize("algo", [gx.PARTITION, gx.PARTITION_GFUR])
+def test_partition_bulk_scatter_matches_register_scatter(monkeypatch, kdt, bits, algo):
+    # Several tiles per SM plus a partial last tile, through the bulk-copy
+    # scatter and through the register scatter (GX_PART_NO_BULK): both must
+    # match the oracle (float sums within tolerance: shared-memory atomics
+    # add in no fixed order).
+    import torch
+    n = 148 * 3 * 4096 + 1234
+    key = O.gen_keys(n, kdt, groups=1 << 16, scatter=1, seed=31)
+    iv = O.gen_values(n, np.int64, lo=-(1 << 40), hi=1 << 40, seed=32)
+    fv = O.gen_values(n, np.float64, seed=33)
+    reqs = [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
+
+    def run(kt, it, ft):
+        hint = gx.make_hint(algo, 1 << 16, radix_bits=bits)
+        return sort_by_key(gx.groupby([kt], [it, ft], reqs, hint).numpy_columns())
+
+    kt, it, ft = to_dev(key), to_dev(iv), to_dev(fv)
+    bulk = run(kt, it, ft)
+    monkeypatch.setenv("GX_PART_NO_BULK", "1")
+    reg = run(kt, it, ft)
+    monkeypatch.delenv("GX_PART_NO_BULK")
+    exp = O.groupby(key, [iv, fv], [(c, OKIND[k]) for c, k in reqs])
+    assert_columns_match(bulk, exp)
+    assert_columns_match(reg, exp)
+    # A value column that starts 8 bytes into its buffer cannot be copied in
+    # 16-byte units: the register scatter takes it, same results.
+    shifted = torch.from_numpy(np.concatenate([np.zeros(1, np.int64), iv])).cuda()[1:]
+    assert shifted.data_ptr() % 16 == 8
+    assert_columns_match(run(kt, shifted, ft), exp)
