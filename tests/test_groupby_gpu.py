@@ -219,3 +219,37 @@ def test_partition_bulk_scatter_matches_register_scatter(monkeypatch, kdt, bits,
     shifted = torch.from_numpy(np.concatenate([np.zeros(1, np.int64), iv])).cuda()[1:]
     assert shifted.data_ptr() % 16 == 8
     assert_columns_match(run(kt, shifted, ft), exp)
+
+
+@pytest.mark.parametrize("order", ["decreasing", "increasing", "mixed"])
+def test_partition_min_max_monotone_values(order):
+    # The unit aggregation reads a group's MIN/MAX and takes the atomic only
+    # when the row moves the extreme.  Monotone values make every late row a
+    # new extreme (or none of them); floats carry NaN, -0.0 / +0.0 and
+    # infinities.
+    n, G = 1 << 20, 4096
+    key = O.gen_keys(n, np.int32, groups=G, scatter=1, seed=41)
+    idx = np.arange(n, dtype=np.int64)
+    if order == "decreasing":
+        iv = -idx * 3 + 7
+    elif order == "increasing":
+        iv = idx * 5 - (1 << 40)
+    else:
+        iv = np.where(idx % 2 == 0, idx, -idx) * 11
+    fv = O.gen_values(n, np.float64, seed=42) + 0.5  # positive: float SUMs without cancellation
+    fv = fv * (1.0 + idx / n) if order != "decreasing" else fv * (2.0 - idx / n)
+    special = np.array([np.nan, -0.0, 0.0, np.inf, -np.inf], dtype=np.float64)
+    pick = (idx % 997) == 0
+    fv[pick] = special[(idx[pick] // 997) % len(special)]
+    reqs = [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
+    hint = gx.make_hint(gx.PARTITION, G)
+    got = sort_by_key(gx.groupby([to_dev(key)], [to_dev(iv), to_dev(fv)], reqs, hint).numpy_columns())
+    exp = O.groupby(key, [iv, fv], [(c, OKIND[k]) for c, k in reqs])
+    # MIN / MAX exact (no rounding is involved).  Float extremes compare by
+    # value: a group holding both zeros may keep either sign (the device
+    # orders -0.0 below +0.0, the oracle keeps the first seen).
+    for c in (2, 3):
+        assert np.array_equal(got[c], exp[c]), c
+    for c in (5, 6):
+        assert np.array_equal(got[c], exp[c], equal_nan=True), c
+    assert_columns_match(got, exp)
