@@ -267,6 +267,11 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
     __shared__ int s_fill, s_spill;
     __shared__ unsigned long long s_base;
     __shared__ int64_t scan_sm[HGB_NT / 32 + 1];
+    // Per-warp queue of rows whose key was not at its home slot: at most 31
+    // left over plus HGB_UNROLL × 32 from one batch.
+    __shared__ uint32_t s_q[HGB_NT / 32][31 + 32 * HGB_UNROLL];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     using kt = typename stable<KW>::kt;
     const kt EMPTY = KW == 4 ? (kt)S_EMPTY4 : (kt)S_EMPTY8;
     stable<KW> st;
@@ -297,6 +302,38 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
         if (threadIdx.x == 0) { s_fill = 0; s_spill = 0; }
         __syncthreads();
         const int64_t tile = (int64_t)HGB_NT * HGB_UNROLL;
+        // One queued row per lane: load it again (cached), walk its probe
+        // sequence, update (or spill to the global table).
+        auto drain = [&](uint32_t off, bool live) {
+            const int64_t i = un.begin + off;
+            uint64_t kq = 0, vq[NV];
+            if (live) {
+                if (KW == 4) kq = canon32(__ldg(static_cast<const unsigned*>(keys) + i), key_kind);
+                else kq = canon64(__ldg(static_cast<const unsigned long long*>(keys) + i), key_kind);
+                if constexpr (sizeof...(ACCS) > 0) {
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) vq[c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < NV; ++c)
+                        if (c < d.n_cols) vq[c] = dev_::load_lane(d.col_ptr[c], d.col_width[c], d.col_kind[c], i);
+                }
+            }
+            const uint32_t hq = live ? key_hash<KW>(kq) : 0u;
+            const int sq = live ? s_find_or_insert<KW>(st, kq, hq >> shift) : -1;
+            __syncwarp();  // regroup after the probe loop (see k_hash_groupby)
+            if (!live) return;
+            if (sq >= 0) {
+                atomicAdd(&my_counts[sq], 1u);
+                if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, sq, vq);
+                else dev_::shared_row_update<NV>(my_acc, s_slots, sq, d, vq);
+            } else {
+                if (!s_spill) s_spill = 1;
+                uint64_t* r = g_find_or_insert<KW>(g, d, kq, hq);
+                if (r) g_update(r, d, vq, 1ull);
+            }
+        };
+        int qfill = 0;
         for (int64_t base = un.begin; base < un.end; base += tile) {
             uint64_t kw[HGB_UNROLL];
             uint64_t v[HGB_UNROLL][NV];
@@ -332,27 +369,32 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
                     if (((volatile kt*)st.keys)[s0] == (kt)kw[q]) slot[q] = (int)s0;
                 }
             }
+            // Rows found at home update now; the others are queued (row
+            // offset in the unit) and walk the probe sequence later, 32 at a
+            // time with every lane busy, instead of holding the whole warp in
+            // a loop for one or two lanes.
 #pragma unroll
             for (int q = 0; q < HGB_UNROLL; ++q) {
-                const bool valid = base + q * HGB_NT + threadIdx.x < un.end;
-                if (valid && slot[q] == -2) slot[q] = s_find_or_insert<KW>(st, kw[q], h[q] >> shift);
-            }
-            __syncwarp();  // regroup after the probe loops (see k_hash_groupby)
-#pragma unroll
-            for (int q = 0; q < HGB_UNROLL; ++q) {
-                const bool valid = base + q * HGB_NT + threadIdx.x < un.end;
-                if (!valid) continue;
-                if (slot[q] >= 0) {
+                const int64_t i = base + q * HGB_NT + threadIdx.x;
+                const bool valid = i < un.end;
+                const bool miss = valid && slot[q] == -2;
+                const unsigned mm = __ballot_sync(0xffffffffu, miss);
+                if (miss) s_q[warp][qfill + __popc(mm & lt)] = (uint32_t)(i - un.begin);
+                qfill += __popc(mm);
+                if (valid && slot[q] >= 0) {
                     atomicAdd(&my_counts[slot[q]], 1u);
                     if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, slot[q], v[q]);
                     else dev_::shared_row_update<NV>(my_acc, s_slots, slot[q], d, v[q]);
-                } else {
-                    if (!s_spill) s_spill = 1;
-                    uint64_t* r = g_find_or_insert<KW>(g, d, kw[q], h[q]);
-                    if (r) g_update(r, d, v[q], 1ull);
                 }
             }
+            __syncwarp();
+            while (qfill >= 32) {
+                qfill -= 32;
+                drain(s_q[warp][qfill + lane], true);
+            }
         }
+        drain(lane < qfill ? s_q[warp][lane] : 0u, lane < qfill);
+        qfill = 0;
         __syncthreads();
         const bool final_groups = !un.split && !s_spill;
         if (final_groups) {
