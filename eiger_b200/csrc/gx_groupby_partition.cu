@@ -283,7 +283,7 @@ constexpr uint32_t PB_WAIT_LIMIT = 1u << 22;
 struct pb_layout {
     uint32_t in_off[MAX_VCOLS + 2];  // column c's slice within one stage
     uint32_t stage_bytes;            // one tile of every loaded column
-    uint32_t whist, qsum, src, sdig, gbase, dbase, total;
+    uint32_t whist, qsum, pk, gbase, dbase, total;
 };
 
 __host__ __device__ inline pb_layout pb_make_layout(const move_cols& mc) {
@@ -297,8 +297,7 @@ __host__ __device__ inline pb_layout pb_make_layout(const move_cols& mc) {
     o *= 2;
     L.whist = o; o += PB_WARPS * PS_BINS * 2;   // u16 per-warp digit counts
     L.qsum = o;  o += 4 * PS_BINS * 2;          // u16 sums over 8-warp quarters
-    L.src = o;   o += PS_TILE * 2;              // u16 source row of each staged position
-    L.sdig = o;  o += PS_TILE;                  // u8 digit of each staged position
+    L.pk = o;    o += PS_TILE * 4;              // u32 per staged position: source row | digit << 16
     L.gbase = o; o += PS_BINS * 8;              // int64 output base per digit
     L.dbase = o; o += PS_BINS * 4;              // u32 first staged position per digit
     L.total = o;
@@ -316,8 +315,7 @@ __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __re
     __shared__ int s_err;
     unsigned short* whist = reinterpret_cast<unsigned short*>(pb_smem + L.whist);
     unsigned short* qsum = reinterpret_cast<unsigned short*>(pb_smem + L.qsum);
-    unsigned short* src = reinterpret_cast<unsigned short*>(pb_smem + L.src);
-    unsigned char* sdig = pb_smem + L.sdig;
+    unsigned* pk = reinterpret_cast<unsigned*>(pb_smem + L.pk);
     int64_t* gbase = reinterpret_cast<int64_t*>(pb_smem + L.gbase);
     unsigned* dbase = reinterpret_cast<unsigned*>(pb_smem + L.dbase);
 
@@ -446,8 +444,7 @@ __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __re
             const int local = warp * 32 * PB_IPT + k * 32 + lane;
             if (local < tile_n) {
                 const unsigned pos = dbase[dig[k]] + whist[warp * PS_BINS + dig[k]] + rank[k];
-                src[pos] = (unsigned short)local;
-                sdig[pos] = (unsigned char)dig[k];
+                pk[pos] = (unsigned)local | (dig[k] << 16);
             }
         }
         __syncthreads();
@@ -455,8 +452,9 @@ __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __re
         for (int m = 0; m < PB_IPT; ++m) {
             const int j = t + m * PB_NT;
             if (j >= tile_n) break;
-            const int64_t orow = gbase[sdig[j]] + j;
-            const int sr = src[j];
+            const unsigned e = pk[j];
+            const int64_t orow = gbase[e >> 16] + j;
+            const int sr = (int)(e & 0xFFFFu);
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
                 if (mc.iota[c]) {
