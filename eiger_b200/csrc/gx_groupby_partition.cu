@@ -304,7 +304,7 @@ __host__ __device__ inline pb_layout pb_make_layout(const move_cols& mc) {
     return L;
 }
 
-template <int KW, int NC>
+template <int KW, int NC, bool STABLE>
 __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __restrict__ keys, int64_t n, int kind,
                                                                 int shift, int dbits, int64_t ntiles,
                                                                 const int64_t* __restrict__ offsets, move_cols mc,
@@ -312,6 +312,7 @@ __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __re
     extern __shared__ __align__(128) unsigned char pb_smem[];
     __shared__ __align__(8) unsigned long long bars[2];
     __shared__ unsigned wsum[PS_BINS / 32];
+    __shared__ unsigned thist[PS_BINS];  // unstable ranking: running count per digit
     __shared__ int s_err;
     unsigned short* whist = reinterpret_cast<unsigned short*>(pb_smem + L.whist);
     unsigned short* qsum = reinterpret_cast<unsigned short*>(pb_smem + L.qsum);
@@ -337,12 +338,21 @@ __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __re
         }
     };
     auto full = [&](int64_t tile) { return (tile + 1) * (int64_t)PS_TILE <= n; };
+    unsigned char* stage = nullptr;
+    // Digit of the tile's row `local` (key column of the current stage).
+    auto digit_at = [&](int local) -> unsigned {
+        uint64_t kb;
+        if (KW == 4) kb = canon32(reinterpret_cast<const unsigned*>(stage + L.in_off[0])[local], kind);
+        else kb = canon64(reinterpret_cast<const unsigned long long*>(stage + L.in_off[0])[local], kind);
+        return (part_hash<KW>(kb) >> shift) & (bins - 1);
+    };
     if (t == 0) {
         dev_::mbar_init(bar0, 1);
         dev_::mbar_init(bar0 + 8, 1);
         dev_::mbar_init_fence();
         s_err = 0;
     }
+    if (t < PS_BINS) thist[t] = 0;
     __syncthreads();
     // A copy into stage b was issued and not yet waited for: tracked by
     // thread 0, the only issuer.
@@ -358,7 +368,7 @@ __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __re
     int it = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const int b = it & 1;
-        unsigned char* stage = pb_smem + (size_t)b * L.stage_bytes;
+        stage = pb_smem + (size_t)b * L.stage_bytes;
         const int64_t tile_base = tile * (int64_t)PS_TILE;
         const int tile_n = (int)min((int64_t)PS_TILE, n - tile_base);
         // Digit offsets of this tile (read early; used after the scan).
@@ -386,47 +396,63 @@ __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __re
             }
             __syncthreads();
         }
-        // Rank: per-warp stable digit counts (rows warp*128 + k*32 + lane).
-        for (int i = lane; i < PS_BINS; i += 32) whist[warp * PS_BINS + i] = 0;
-        __syncwarp();
+        // Rank the tile's rows within their digit.  STABLE (every pass after
+        // the first of a multi-pass partition, which LSD order needs): per-warp
+        // counts over rows warp*128 + k*32 + lane, then a cross-warp prefix.
+        // Otherwise one shared atomic per row gives an arbitrary order within
+        // each (digit, tile) run, which a single-pass partition allows.
         unsigned dig[PB_IPT], rank[PB_IPT];
+        unsigned tot = 0, incl = 0;
+        if constexpr (STABLE) {
+            for (int i = lane; i < PS_BINS; i += 32) whist[warp * PS_BINS + i] = 0;
+            __syncwarp();
 #pragma unroll
-        for (int k = 0; k < PB_IPT; ++k) {
-            const int local = warp * 32 * PB_IPT + k * 32 + lane;
-            const bool valid = local < tile_n;
-            uint64_t kb = 0;
-            if (valid) {
-                if (KW == 4) kb = canon32(reinterpret_cast<const unsigned*>(stage + L.in_off[0])[local], kind);
-                else kb = canon64(reinterpret_cast<const unsigned long long*>(stage + L.in_off[0])[local], kind);
+            for (int k = 0; k < PB_IPT; ++k) {
+                const int local = warp * 32 * PB_IPT + k * 32 + lane;
+                const bool valid = local < tile_n;
+                const unsigned d = valid ? digit_at(local) : 0xFFFFu;
+                dig[k] = d;
+                const unsigned peers = __match_any_sync(0xffffffffu, d);
+                const unsigned r = __popc(peers & lt);
+                const unsigned prior = valid ? whist[warp * PS_BINS + d] : 0;
+                rank[k] = prior + r;
+                __syncwarp();
+                if (valid && r == 0) whist[warp * PS_BINS + d] = (unsigned short)(prior + __popc(peers));
+                __syncwarp();
             }
-            const unsigned d = valid ? (part_hash<KW>(kb) >> shift) & (bins - 1) : 0xFFFFu;
-            dig[k] = d;
-            const unsigned peers = __match_any_sync(0xffffffffu, d);
-            const unsigned r = __popc(peers & lt);
-            const unsigned prior = valid ? whist[warp * PS_BINS + d] : 0;
-            rank[k] = prior + r;
-            __syncwarp();
-            if (valid && r == 0) whist[warp * PS_BINS + d] = (unsigned short)(prior + __popc(peers));
-            __syncwarp();
+            __syncthreads();
+            if (s_err) break;
+            // Cross-warp exclusive prefix per digit: thread (q, bin) sums warps 8q..8q+7.
+            const int bq = t & (PS_BINS - 1), q = t >> 8;
+            unsigned v[8], s = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) { v[j] = whist[(q * 8 + j) * PS_BINS + bq]; s += v[j]; }
+            qsum[q * PS_BINS + bq] = (unsigned short)s;
+            __syncthreads();
+            unsigned run = 0;
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) {
+                const unsigned x = qsum[qq * PS_BINS + bq];
+                if (qq < q) run += x;
+                tot += x;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) { whist[(q * 8 + j) * PS_BINS + bq] = (unsigned short)run; run += v[j]; }
+        } else {
+#pragma unroll
+            for (int k = 0; k < PB_IPT; ++k) {
+                const int local = warp * 32 * PB_IPT + k * 32 + lane;
+                const bool valid = local < tile_n;
+                dig[k] = valid ? digit_at(local) : 0u;
+                rank[k] = valid ? atomicAdd(&thist[dig[k]], 1u) : 0u;
+            }
+            __syncthreads();
+            if (s_err) break;
+            if (t < PS_BINS) {
+                tot = thist[t];
+                thist[t] = 0;  // ready for the next tile
+            }
         }
-        __syncthreads();
-        if (s_err) break;
-        // Cross-warp exclusive prefix per digit: thread (q, bin) sums warps 8q..8q+7.
-        const int bq = t & (PS_BINS - 1), q = t >> 8;
-        unsigned v[8], s = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) { v[j] = whist[(q * 8 + j) * PS_BINS + bq]; s += v[j]; }
-        qsum[q * PS_BINS + bq] = (unsigned short)s;
-        __syncthreads();
-        unsigned run = 0, tot = 0, incl = 0;
-#pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-            const unsigned x = qsum[qq * PS_BINS + bq];
-            if (qq < q) run += x;
-            tot += x;
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) { whist[(q * 8 + j) * PS_BINS + bq] = (unsigned short)run; run += v[j]; }
         if (t < PS_BINS) {
             incl = dev_::warp_inclusive_sum(tot);
             if (lane == 31) wsum[warp] = incl;
@@ -443,7 +469,7 @@ __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __re
         for (int k = 0; k < PB_IPT; ++k) {
             const int local = warp * 32 * PB_IPT + k * 32 + lane;
             if (local < tile_n) {
-                const unsigned pos = dbase[dig[k]] + whist[warp * PS_BINS + dig[k]] + rank[k];
+                const unsigned pos = dbase[dig[k]] + (STABLE ? (unsigned)whist[warp * PS_BINS + dig[k]] : 0u) + rank[k];
                 pk[pos] = (unsigned)local | (dig[k] << 16);
             }
         }
@@ -775,12 +801,12 @@ static bool bulk_scatter_ok(const move_cols& mc, const pb_layout& L) {
         if (mc.width[c] != 4 && mc.width[c] != 8) return false;
         if (reinterpret_cast<uintptr_t>(mc.in[c]) % 16 != 0) return false;
     }
-    return L.total <= (uint32_t)dev().max_smem_optin - 1024;
+    return L.total <= (uint32_t)dev().max_smem_optin - 2048;
 }
 
 template <int KW>
 void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_cols& mc, int64_t* counts,
-               int64_t* offs, int* err, cudaStream_t s) {
+               int64_t* offs, int* err, bool stable, cudaStream_t s) {
     int64_t ntiles = ceil_div(n, PS_TILE);
     const int hist_grid = (int)std::min<int64_t>(ceil_div(ntiles, PH_WARPS), (int64_t)dev().sm_count * 8);
     k_part_hist<KW><<<hist_grid, PH_NT, 0, s>>>(kin, n, kind, shift, dbits, ntiles, counts);
@@ -790,18 +816,22 @@ void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_
     if (bulk_scatter_ok(mc, L)) {
         static bool battr[16] = {};
         if (!battr[dev().device]) {
-            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         dev().max_smem_optin - 1024));
-            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         dev().max_smem_optin - 1024));
+            const int lim = dev().max_smem_optin - 2048;
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             battr[dev().device] = true;
         }
         const int grid = (int)std::min<int64_t>(ntiles, dev().sm_count);
         GX_PROF("partition_scatter", s);
-        if (mc.n == 2)
-            k_part_scatter_bulk<KW, 2><<<grid, PB_NT, L.total, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc, L, err);
-        else
-            k_part_scatter_bulk<KW, 3><<<grid, PB_NT, L.total, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc, L, err);
+#define GX_PB_LAUNCH(NCV, ST) \
+    k_part_scatter_bulk<KW, NCV, ST><<<grid, PB_NT, L.total, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc, L, err)
+        if (mc.n == 2 && stable) GX_PB_LAUNCH(2, true);
+        else if (mc.n == 2) GX_PB_LAUNCH(2, false);
+        else if (stable) GX_PB_LAUNCH(3, true);
+        else GX_PB_LAUNCH(3, false);
+#undef GX_PB_LAUNCH
         GX_LAUNCHED();
         return;
     }
@@ -900,8 +930,10 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
                 for (int c = 0; c < mc.n; ++c) { m.in[c] = bufs_b[c].get(); m.iota[c] = 0; m.out[c] = bufs_a[c].get(); }
             }
             const void* kin = m.in[0];
-            if (kw == 4) part_pass<4>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr.get<int>(), s);
-            else part_pass<8>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr.get<int>(), s);
+            // Only the first digit pass may leave rows unordered within a run.
+            const bool stable = ps > 0;
+            if (kw == 4) part_pass<4>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr.get<int>(), stable, s);
+            else part_pass<8>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr.get<int>(), stable, s);
             shift += dbits;
         }
     }
