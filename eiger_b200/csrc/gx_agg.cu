@@ -191,7 +191,9 @@ __global__ void __launch_bounds__(EMIT_NT) k_emit_write(emit_args a, const int64
     int64_t r = blockIdx.x * (int64_t)EMIT_NT + threadIdx.x;
     bool live = r < a.nrec && rec_live(a, r);
     int64_t total;
-    int64_t pos = dev_::block_exclusive_sum<EMIT_NT, int64_t>(live ? 1 : 0, sm, &total) + blk_off[blockIdx.x];
+    // Dense records (no compaction) sit at their own index.
+    const int64_t base = a.compact ? blk_off[blockIdx.x] : blockIdx.x * (int64_t)EMIT_NT;
+    int64_t pos = dev_::block_exclusive_sum<EMIT_NT, int64_t>(live ? 1 : 0, sm, &total) + base;
     if (!live) return;
     const uint64_t* rec = a.recs + r * a.rec_words;
     uint64_t kb = rec[0];
@@ -236,10 +238,13 @@ void emit_groupby_output(const agg_plan& p, const uint64_t* recs, int64_t nrec, 
     a.n_out = (int)p.outs.size();
     int64_t nblk = ceil_div(nrec > 0 ? nrec : 1, EMIT_NT);
     dbuf blk(nblk * sizeof(int64_t), s), off((nblk + 1) * sizeof(int64_t), s);
-    k_emit_count<<<(unsigned)nblk, EMIT_NT, 0, s>>>(a, blk.get<int64_t>());
-    GX_LAUNCHED();
-    exclusive_scan_i64(blk.get<int64_t>(), off.get<int64_t>(), nblk, s);
-    int64_t groups = read_scalar(off.get<int64_t>() + nblk, s);
+    int64_t groups = nrec;
+    if (compact) {
+        k_emit_count<<<(unsigned)nblk, EMIT_NT, 0, s>>>(a, blk.get<int64_t>());
+        GX_LAUNCHED();
+        exclusive_scan_i64(blk.get<int64_t>(), off.get<int64_t>(), nblk, s);
+        groups = read_scalar(off.get<int64_t>() + nblk, s);
+    }
     int64_t cap = std::max<int64_t>(groups, std::min<int64_t>(out_capacity, groups));
     out->cols.clear();
     out->cols.push_back(make_col(key_type, groups, s, cap));

@@ -913,8 +913,11 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
 
     int64_t ntiles = ceil_div(std::max<int64_t>(n, 1), PS_TILE);
     dbuf counts((size_t)PS_BINS * ntiles * 8, s), offs((size_t)PS_BINS * ntiles * 8 + 8, s);
-    dbuf perr(sizeof(int), s);  // set by the bulk-copy scatter when a copy wait gave up
-    GX_CUDA(cudaMemsetAsync(perr.get(), 0, sizeof(int), s));
+    // Unit offsets [0, P] then one word the bulk-copy scatter sets when a
+    // copy wait gave up, so one read after the unit setup fetches both.
+    dbuf uoff((size_t)(P + 2) * 8, s);
+    int* perr = reinterpret_cast<int*>(uoff.get<int64_t>() + P + 1);
+    GX_CUDA(cudaMemsetAsync(perr, 0, 8, s));
     int passes = (R + 7) / 8;
     // Two digit passes ping-pong between bufs_a and bufs_b.
     if (passes == 2)
@@ -932,8 +935,8 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
             const void* kin = m.in[0];
             // Only the first digit pass may leave rows unordered within a run.
             const bool stable = ps > 0;
-            if (kw == 4) part_pass<4>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr.get<int>(), stable, s);
-            else part_pass<8>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr.get<int>(), stable, s);
+            if (kw == 4) part_pass<4>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr, stable, s);
+            else part_pass<8>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr, stable, s);
             shift += dbits;
         }
     }
@@ -955,7 +958,7 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     // hot partitions), and with few partitions every partition is split so
     // that about four units per SM exist.
     int64_t T = std::max<int64_t>(1 << 14, std::min<int64_t>(2 * ceil_div(n, P), ceil_div(n, (int64_t)dev().sm_count * 8)));
-    dbuf ucount((size_t)P * 8, s), uoff((size_t)(P + 1) * 8, s);
+    dbuf ucount((size_t)P * 8, s);
     k_unit_counts<<<(unsigned)ceil_div(P, 256), 256, 0, s>>>(pstart.get<int64_t>(), P, T, ucount.get<int64_t>());
     GX_LAUNCHED();
     exclusive_scan_i64(ucount.get<int64_t>(), uoff.get<int64_t>(), P, s);
@@ -968,8 +971,11 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     uint64_t empty = kw == 4 ? PG_EMPTY4 : PG_EMPTY8;
     // Split units merge through the spill table, so size it for every group
     // when any partition was split; otherwise it only catches overflow.
-    int64_t total_units = read_scalar(uoff.get<int64_t>() + P, s);
-    if (read_scalar(perr.get<int>(), s)) fail(GX_ETIMEOUT, "partition scatter: a bulk copy into shared memory did not complete");
+    int64_t tail[2];
+    GX_CUDA(cudaMemcpyAsync(tail, uoff.get<int64_t>() + P, sizeof(tail), cudaMemcpyDeviceToHost, s));
+    GX_CUDA(cudaStreamSynchronize(s));
+    const int64_t total_units = tail[0];
+    if ((int)tail[1]) fail(GX_ETIMEOUT, "partition scatter: a bulk copy into shared memory did not complete");
     int64_t live_parts = std::min<int64_t>(P, n);
     uint64_t gcap = 1u << 16;
     // Also when partitions hold more groups than a shared table (radix bits
@@ -1021,15 +1027,21 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
             }
             GX_LAUNCHED();
         }
-        int ovf = read_scalar(flags.get<int>() + 1, s);
-        if (ovf) { gcap *= 8; continue; }
+        // The spill records are appended before the overflow flags are read,
+        // so one read decides: a spill-table overflow discards this attempt.
         k_append_global<<<grid_for((int64_t)gcap + 1, 256, 4), 256, 0, s>>>(grec.get<uint64_t>(), (int64_t)gcap,
                                                                           d.rec_words, empty, flags.get<int>(),
                                                                           orec.get<uint64_t>(), ocount, rec_cap,
                                                                           rec_ovf);
         GX_LAUNCHED();
-        int64_t groups = (int64_t)read_scalar(ocount, s);
-        if (read_scalar(rec_ovf, s)) {
+        int fl[8];
+        GX_CUDA(cudaMemcpyAsync(fl, flags.get(), sizeof(fl), cudaMemcpyDeviceToHost, s));
+        GX_CUDA(cudaStreamSynchronize(s));
+        if (fl[1]) { gcap *= 8; continue; }
+        unsigned long long ocount_h;
+        std::memcpy(&ocount_h, reinterpret_cast<const char*>(fl) + 8, 8);
+        const int64_t groups = (int64_t)ocount_h;
+        if (fl[4]) {
             rec_cap = std::min<int64_t>(std::max<int64_t>(n, 1), rec_cap * 4);
             continue;
         }
