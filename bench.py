@@ -219,8 +219,20 @@ def run_gx(args) -> None:
     achieved = kernel_bytes[main_kernel] / (k_launch_ms * 1e-3) / 1e9 if kcnt else None
     algo_name = {gx.HASH: "hash", gx.SORT: "sort", gx.SORT_OPT: "sort_opt", gx.SORT_GFUR: "sort_gfur",
                  gx.PARTITION: "partition", gx.PARTITION_GFUR: "partition_gfur"}.get(chosen.get("algo"), "?")
+    # DRAM bytes per row of the partition plan's two kernels on this workload,
+    # from one ncu capture at 2^25 rows (dram__bytes_read.sum + dram__bytes_write.sum
+    # per launch ÷ 2^25; DRAM bytes grow in proportion to rows), scaled to this run:
+    #   ncu --set full --clock-control none -k regex:"k_hash_units|k_part_scatter_bulk" -s 2 -c 2 \
+    #       python bench.py --rows 33554432 --steps 3 --warmup 3 --no-join --batch-instances 0 --no-cpu
+    # k_hash_units 678.12 + 8.59 MB, k_part_scatter_bulk 688.36 + 621.05 MB (the scatter's
+    # last writes leave L2 after the kernel ends).
+    dram_per_row = {"partition_aggregate": (678.12e6 + 8.59e6) / 2**25,
+                    "partition_scatter": (688.36e6 + 621.05e6) / 2**25}
+    traffic = args.traffic
+    if traffic is None and main_kernel in dram_per_row and G == 1 << 16 and algo_name.startswith("partition"):
+        traffic = dram_per_row[main_kernel] * rows
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": args.traffic,
+                "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": traffic,
                 "kernel": main_kernel, "kernel_ms": k_launch_ms, "launches_per_step": kcnt / prof_steps,
                 "kernel_share_of_step": kms / prof_steps / max(ms_step, 1e-9), "peak_source": peaks["source"],
                 "kernels_ms_per_step": {nm: round(t / prof_steps, 4) for nm, (t, c) in kstats.items() if c},
