@@ -269,11 +269,12 @@ __global__ void __launch_bounds__(PS_NT, 2) k_part_scatter_r(const void* __restr
 // + gridDim.x, ...), with each tile's column slices brought into shared
 // memory by the copy engine (cp.async.bulk on an mbarrier) one tile ahead, so
 // the loads of tile t+1 overlap the ranking and writes of tile t and no
-// column value occupies a register.  A tile is ranked exactly as in
-// k_part_scatter (stable: digit, then row order), then each output position
-// j reads its source row from the shared copy and writes every column to
-// gbase[digit] + j.  Used when every loaded column starts on a 16-byte
-// boundary and two tiles of the columns fit in shared memory.
+// column value occupies a register.  STABLE ranks a tile as k_part_scatter
+// does (digit, then row order); otherwise each row's rank within its digit
+// is one shared atomic (any order inside a (digit, tile) run).  Each output
+// position j then reads its source row from the shared copy and writes every
+// column to gbase[digit] + j.  Used when every loaded column starts on a
+// 16-byte boundary and two tiles of the columns fit in shared memory.
 // ---------------------------------------------------------------------------
 constexpr int PB_NT = 1024;
 constexpr int PB_WARPS = PB_NT / 32;
