@@ -137,9 +137,12 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restri
                                                              uint32_t s_slots, int reps) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_fill;
+    // Per-warp queue of a batch's rows whose key was not at its home slot.
+    __shared__ unsigned short s_bq[SMEM ? HGB_NT / 32 : 1][SMEM ? 32 * HGB_UNROLL : 1];
     stable<KW> st;
     using kt = typename stable<KW>::kt;
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     unsigned* my_counts = nullptr;
     uint64_t* my_acc = nullptr;
     if (SMEM) {
@@ -192,27 +195,74 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restri
                 }
             }
         }
+        if constexpr (SMEM) {
+            // Home-slot probe of every row of the batch at once; rows found
+            // there update now, the others are queued (offset in the batch)
+            // and walk the probe sequence together at the end of the batch.
+            const kt EMPTY = KW == 4 ? (kt)S_EMPTY4 : (kt)S_EMPTY8;
+            int qfill = 0;
 #pragma unroll
-        for (int u = 0; u < HGB_UNROLL; ++u) {
-            const int64_t i = base + u * HGB_NT + threadIdx.x;
-            const bool valid = i < n;
-            uint32_t h = 0;
-            int slot = -1;
-            if (valid) {
-                h = key_hash<KW>(kw[u]);
-                if (SMEM) slot = s_find_or_insert<KW>(st, kw[u], h);
+            for (int u = 0; u < HGB_UNROLL; ++u) {
+                const int off = u * HGB_NT + (int)threadIdx.x;
+                const bool valid = base + off < n;
+                const uint32_t h = valid ? key_hash<KW>(kw[u]) : 0u;
+                int slot = -2;
+                if (valid && (kt)kw[u] != EMPTY) {
+                    const uint32_t s0 = h & st.mask;
+                    if (((volatile kt*)st.keys)[s0] == (kt)kw[u]) slot = (int)s0;
+                }
+                const bool miss = valid && slot == -2;
+                const unsigned mm = __ballot_sync(0xffffffffu, miss);
+                if (miss) s_bq[warp][qfill + __popc(mm & lt)] = (unsigned short)off;
+                qfill += __popc(mm);
+                if (valid && slot >= 0) {
+                    // The per-replica count is kept even without COUNT: it
+                    // tells the merge which replicas saw the group (for ANY).
+                    atomicAdd(&my_counts[slot], 1u);
+                    if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, slot, v[u]);
+                    else dev_::shared_row_update<NV>(my_acc, s_slots, slot, d, v[u]);
+                }
             }
-            // Lanes leave the probe loop at different steps; regroup the warp
-            // so the updates below issue once per warp, not once per exit step.
             __syncwarp();
-            if (!valid) continue;
-            if (slot >= 0) {
-                // The per-replica count is kept even without COUNT: it tells
-                // the merge which replicas saw the group (for ANY).
-                atomicAdd(&my_counts[slot], 1u);
-                if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, slot, v[u]);
-                else dev_::shared_row_update<NV>(my_acc, s_slots, slot, d, v[u]);
-            } else {
+            for (int q0 = 0; q0 < qfill; q0 += 32) {
+                const bool live = q0 + lane < qfill;
+                const int64_t i = base + (live ? s_bq[warp][q0 + lane] : 0);
+                uint64_t kq = 0, vq[NV];
+                if (live) {
+                    if (KW == 4) kq = canon32(__ldg(static_cast<const unsigned*>(keys) + i), key_kind);
+                    else kq = canon64(__ldg(static_cast<const unsigned long long*>(keys) + i), key_kind);
+                    if constexpr (sizeof...(ACCS) > 0) {
+#pragma unroll
+                        for (int c = 0; c < NV; ++c) vq[c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NV; ++c)
+                            if (c < d.n_cols) vq[c] = dev_::load_lane(d.col_ptr[c], d.col_width[c], d.col_kind[c], i);
+                    }
+                }
+                const uint32_t hq = live ? key_hash<KW>(kq) : 0u;
+                const int sq = live ? s_find_or_insert<KW>(st, kq, hq) : -1;
+                // Lanes leave the probe loop at different steps; regroup the
+                // warp so the updates issue once per warp, not once per exit step.
+                __syncwarp();
+                if (live) {
+                    if (sq >= 0) {
+                        atomicAdd(&my_counts[sq], 1u);
+                        if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, sq, vq);
+                        else dev_::shared_row_update<NV>(my_acc, s_slots, sq, d, vq);
+                    } else {
+                        uint64_t* r = g_find_or_insert<KW>(g, d, kq, hq);
+                        if (r) g_update(r, d, vq, 1ull);
+                    }
+                }
+                __syncwarp();
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < HGB_UNROLL; ++u) {
+                const int64_t i = base + u * HGB_NT + threadIdx.x;
+                if (i >= n) continue;
+                const uint32_t h = key_hash<KW>(kw[u]);
                 uint64_t* r = g_find_or_insert<KW>(g, d, kw[u], h);
                 if (r) g_update(r, d, v[u], 1ull);
             }
