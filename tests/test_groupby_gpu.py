@@ -253,3 +253,45 @@ def test_partition_min_max_monotone_values(order):
     for c in (5, 6):
         assert np.array_equal(got[c], exp[c], equal_nan=True), c
     assert_columns_match(got, exp)
+
+
+@pytest.mark.parametrize("env,algo,G", [
+    ("GX_HASH_GENERIC", gx.HASH, 4096),      # run-time aggregation list instead of a compiled plan
+    ("GX_HASH_GENERIC", gx.PARTITION, 1 << 16),
+    ("GX_PART_OLD_AGG", gx.PARTITION, 1 << 16),  # per-partition CTA aggregation kernel
+])
+def test_forced_alternative_kernels(monkeypatch, env, algo, G):
+    # The switches route a plan through its alternative kernel; results must
+    # not change.
+    n = 1 << 19
+    key = O.gen_keys(n, np.int32, groups=G, scatter=1, seed=51)
+    iv = O.gen_values(n, np.int64, lo=-(1 << 35), hi=1 << 35, seed=52)
+    fv = O.gen_values(n, np.float64, seed=53)
+    reqs = [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
+    monkeypatch.setenv(env, "1")
+    got, exp, _ = run_both(key, [iv, fv], reqs, algo, bound=G)
+    assert_columns_match(got, exp)
+
+
+@pytest.mark.parametrize("smem", ["0", "1"])
+def test_hash_table_mode_forced(monkeypatch, smem):
+    # GX_HASH_SMEM forces the HASH plan's shared-table mode on or off (global
+    # L2-resident record table only).
+    n = 1 << 19
+    key = O.gen_keys(n, np.int64, groups=3000, scatter=1, seed=61)
+    val = O.gen_values(n, np.int64, lo=0, hi=1 << 20, seed=62)
+    monkeypatch.setenv("GX_HASH_SMEM", smem)
+    got, exp, _ = run_both(key, [val], [(0, gx.SUM), (0, gx.MAX), (0, gx.COUNT_ALL)], gx.HASH, bound=3000)
+    assert_columns_match(got, exp)
+
+
+def test_partition_groups_per_partition_override(monkeypatch):
+    # GX_PART_GROUPS sets the target groups per partition (here 16: more radix
+    # bits, two digit passes at this group count).
+    n = 1 << 19
+    key = O.gen_keys(n, np.int32, groups=1 << 16, scatter=1, seed=71)
+    val = O.gen_values(n, np.int64, lo=0, hi=1000, seed=72)
+    monkeypatch.setenv("GX_PART_GROUPS", "16")
+    got, exp, hint = run_both(key, [val], [(0, gx.SUM), (0, gx.COUNT_ALL)], gx.PARTITION, bound=1 << 16)
+    assert hint.radix_bits == 12
+    assert_columns_match(got, exp)
