@@ -345,8 +345,8 @@ def run_gx(args) -> None:
         torch.cuda.empty_cache()
 
     # ------------------------------------------------------ cpu baseline
-    cpu = None
-    if rank == 0 and not args.no_cpu:
+    cpu = None  # timed on rank 0 of single-GPU runs only
+    if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_groupby_baseline(args.cpu_rows, G)
 
     if rank == 0:
