@@ -54,7 +54,7 @@ typedef enum gx_status {
     GX_ECUDA = 3,        /* a CUDA runtime call failed */
     GX_EOVERFLOW = 4,    /* a capacity (table, output buffer, batch) was exceeded */
     GX_ETIMEOUT = 5,     /* a bounded device-side wait gave up */
-    GX_EUNSUPPORTED = 6  /* valid request this build does not implement */
+    GX_EUNSUPPORTED = 6  /* valid request this library does not implement */
 } gx_status;
 
 typedef enum gx_sort_order { GX_ASCENDING = 0, GX_DESCENDING = 1 } gx_sort_order;
