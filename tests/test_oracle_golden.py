@@ -187,3 +187,47 @@ def test_generators_cyclic_exact_and_hll():
     est = O.hll_estimate(O.hll_registers(big))
     exact = O.ndv_exact(big)
     assert abs(est - exact) / exact < 0.04
+
+
+@pytest.mark.parametrize("vdt", [np.int8, np.int16, np.int32, np.uint32, np.int64, np.uint64, np.float32, np.float64])
+def test_groupby_value_types_against_numpy(vdt):
+    # Output types follow the reference (agg_func.cuh:20-60): integer SUM
+    # widens to 64 bits (signedness kept), float SUM keeps the float type
+    # (accumulated in higher precision, rounded once), MIN/MAX keep the input
+    # type, AVG is double, COUNT int64.
+    n = 4000
+    k = O.gen_keys(n, np.int32, groups=37, scatter=1, seed=21)
+    if np.dtype(vdt).kind == "f":
+        v = ((O.gen_values(n, np.float64, seed=22) - 0.5) * 100).astype(vdt)
+    else:
+        info = np.iinfo(vdt)
+        v = O.gen_values(n, np.int64, lo=max(int(info.min), -(1 << 30)), hi=min(int(info.max), 1 << 30),
+                         seed=22).astype(vdt)
+    out = O.groupby(k, [v], [(0, O.SUM), (0, O.MIN), (0, O.MAX), (0, O.AVG), (0, O.COUNT_ALL)])
+    for i, key in enumerate(out[0]):
+        m = k == key
+        x = v[m]
+        if np.dtype(vdt).kind == "f":
+            rtol = 1e-6 if vdt == np.float32 else 1e-12
+            ref = x.astype(np.float64).sum()
+            assert out[1].dtype == vdt
+            assert abs(float(out[1][i]) - ref) <= rtol * max(1.0, abs(ref))
+        else:
+            assert int(out[1][i]) == int(x.astype(np.int64 if np.dtype(vdt).kind == "i" else np.uint64).sum())
+        assert out[2][i] == x.min() and out[3][i] == x.max()
+        assert out[2].dtype == vdt and out[3].dtype == vdt
+        assert abs(out[4][i] - x.astype(np.float64).mean()) <= 1e-9 * max(1.0, abs(x.astype(np.float64).mean()))
+        assert out[5][i] == m.sum()
+
+
+def test_groupby_float_nan_semantics():
+    # NaN takes part in SUM (the sum becomes NaN) but not in MIN/MAX; a group
+    # of NaNs only keeps the identities.
+    k = np.array([1, 1, 1, 2, 2, 3], dtype=np.int32)
+    v = np.array([1.5, np.nan, -2.0, np.nan, np.nan, 4.0], dtype=np.float64)
+    out = O.groupby(k, [v], [(0, O.SUM), (0, O.MIN), (0, O.MAX), (0, O.COUNT_ALL)])
+    assert list(out[0]) == [1, 2, 3]
+    assert np.isnan(out[1][0]) and np.isnan(out[1][1]) and out[1][2] == 4.0
+    assert out[2][0] == -2.0 and out[3][0] == 1.5
+    assert out[2][2] == 4.0 and out[3][2] == 4.0
+    assert list(out[4]) == [3, 2, 1]
