@@ -124,3 +124,46 @@ int main() {
     assert out[0].startswith("caught:") and "auto selection" in out[0]
     algo, sum_type, bound = out[1].split()
     assert int(algo) == 0 and int(sum_type) == int(gx.INT64) and int(bound) == 2 ** 63 - 1
+
+
+def test_invalid_arguments_are_rejected_with_messages():
+    # Host-side validation, the reference's std::runtime_error cases
+    # (groupby.cu:68-120, sort.cu, partition.cu, stats_compute.cu): each call
+    # returns GX_EINVAL with a message and does no device work.
+    cv = gx.ColumnView
+
+    def table(cols):
+        arr = (cv * len(cols))(*cols)
+        return gx.TableView(arr, len(cols)), arr
+
+    out = ctypes.c_void_p()
+    kt, _k = table([cv(None, 10, gx.INT32, 0)])
+    short_vt, _v = table([cv(None, 9, gx.INT64, 0)])
+    vt, _w = table([cv(None, 10, gx.INT64, 0)])
+    req = (gx.AggRequest * 1)(gx.AggRequest(0, gx.SUM))
+    bad_req = (gx.AggRequest * 1)(gx.AggRequest(5, gx.SUM))
+
+    def groupby(vals, reqs, algo=gx.HASH):
+        h = gx.make_hint(gx.HASH, 10)
+        h.groupby_algo = algo
+        return gx.lib.gx_groupby(ctypes.byref(kt), ctypes.byref(vals), reqs, 1, ctypes.byref(h), None,
+                                 ctypes.byref(out))
+
+    oc, ko, vo = gx.OwnedColumn(), gx.OwnedColumn(), gx.OwnedColumn()
+    ndv = ctypes.c_int64()
+    cases = [
+        (lambda: groupby(short_vt, req), "different row count"),
+        (lambda: groupby(vt, req, algo=99), "Unsupported groupby algorithm"),
+        (lambda: groupby(vt, bad_req), "out of range"),
+        (lambda: gx.lib.gx_compute_partition_offsets(cv(None, 10, gx.INT32, 0), 0, 40, None, ctypes.byref(oc)),
+         "bad bit range"),
+        (lambda: gx.lib.gx_compute_ndv_approx(cv(None, 10, gx.STRING, 0), None, ctypes.byref(ndv)),
+         "unsupported column type"),
+        (lambda: gx.lib.gx_sort_column_pair(cv(None, 10, gx.INT32, 0), cv(None, 10, gx.INT64, 0), 0, -1, 7, None, 0,
+                                            None, ctypes.byref(ko), ctypes.byref(vo)), "bad order"),
+        (lambda: gx.lib.gx_sort_column_pair(cv(None, 10, gx.STRING, 0), cv(None, 10, gx.INT64, 0), 0, -1, 0, None, 0,
+                                            None, ctypes.byref(ko), ctypes.byref(vo)), "unsupported key type"),
+    ]
+    for call, words in cases:
+        assert call() == 1, words
+        assert words in gx.last_error()
