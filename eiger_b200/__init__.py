@@ -113,7 +113,7 @@ class BatchResult(C.Structure):
 def _load() -> C.CDLL:
     path = os.environ.get("GX_LIB", str(_LIB_PATH))
     if not Path(path).exists():
-        raise ImportError(f"libgx.so not found at {path}; build it with `python -m eiger_b200.build`")
+        raise ImportError(f"libgx.so not found at {path}; build it with `python eiger_b200/build.py`")
     lib = C.CDLL(path)
     vp, i32, i64, f64 = C.c_void_p, C.c_int32, C.c_int64, C.c_double
     tv, cv = C.POINTER(TableView), ColumnView
