@@ -80,8 +80,10 @@ struct prof_scope {
 void prof_read(const char* name, double* total_ms, int64_t* count, bool reset);
 
 // ---------------------------------------------------------------------------
-// Device properties (cached per device).
+// Device properties (cached per device).  Device ordinals at or above
+// GX_MAX_DEVICES are rejected with GX_EUNSUPPORTED by dev().
 // ---------------------------------------------------------------------------
+constexpr int GX_MAX_DEVICES = 64;
 struct device_info {
     int device = 0;
     int sm_count = 148;
@@ -89,6 +91,21 @@ struct device_info {
     int l2_bytes = 126 * 1024 * 1024;
 };
 const device_info& dev();
+
+// One-time per-device set-up (kernel attributes and the like), safe to call
+// from several host threads: `fn` runs on the current device until one call
+// returns normally, after which the device's flag stays set.  Two threads
+// may both run `fn` the first time, so `fn` must be idempotent.
+struct per_device_flag {
+    std::atomic<bool> set[GX_MAX_DEVICES] = {};
+    template <class F>
+    void once(F&& fn) {
+        const int d = dev().device;
+        if (set[d].load(std::memory_order_acquire)) return;
+        fn();
+        set[d].store(true, std::memory_order_release);
+    }
+};
 
 // ---------------------------------------------------------------------------
 // Stream-ordered pool allocator (cudaMallocAsync on the device's default

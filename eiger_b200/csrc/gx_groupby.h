@@ -54,6 +54,9 @@ void radix_sort(const col& keys, const void* vals_in, int val_width, bool vals_i
 size_t radix_pairs_scratch_bytes(int64_t n, int key_width, int val_width);
 void radix_sort_pairs_scratch(const col& keys, const void* vals_in, int val_width, int begin_bit, int end_bit,
                               bool descending, void* keys_out, void* vals_out, char* scratch, cudaStream_t s);
+// Sets, on the current device, the kernel attributes every 4/8-byte pair
+// scatter needs (each is otherwise set before its first launch).
+void radix_prepare_pair_scatters();
 // Key image width in bits for a type (the default end_bit).
 inline int key_bits(int type) { return 8 * size_of(type); }
 

@@ -815,15 +815,14 @@ void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_
     exclusive_scan_i64(counts, offs, ((int64_t)1 << dbits) * ntiles, s);
     const pb_layout L = pb_make_layout(mc);
     if (bulk_scatter_ok(mc, L)) {
-        static bool battr[16] = {};
-        if (!battr[dev().device]) {
+        static per_device_flag battr;
+        battr.once([] {
             const int lim = dev().max_smem_optin - 2048;
             GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-            battr[dev().device] = true;
-        }
+        });
         const int grid = (int)std::min<int64_t>(ntiles, dev().sm_count);
         GX_PROF("partition_scatter", s);
 #define GX_PB_LAUNCH(NCV, ST) \
@@ -837,13 +836,12 @@ void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_
         return;
     }
     const int dyn = PS_TILE * 10;
-    static bool attr[16] = {};
-    if (!attr[dev().device]) {
+    static per_device_flag attr;
+    attr.once([dyn] {
         GX_CUDA(cudaFuncSetAttribute(k_part_scatter<KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
         GX_CUDA(cudaFuncSetAttribute(k_part_scatter_r<KW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
         GX_CUDA(cudaFuncSetAttribute(k_part_scatter_r<KW, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
-        attr[dev().device] = true;
-    }
+    });
     GX_PROF("partition_scatter", s);
     if (mc.n == 2) k_part_scatter_r<KW, 2><<<(unsigned)ntiles, PS_NT, dyn, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc);
     else if (mc.n == 3) k_part_scatter_r<KW, 3><<<(unsigned)ntiles, PS_NT, dyn, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc);

@@ -24,10 +24,12 @@
 //     them, or concurrent host threads on different streams) race and corrupt
 //     each other's results; order them on one stream or with events;
 //   * the first call on each device resolves the array's device address with
-//     cudaGetSymbolAddress (which may load this file's device code) and sets
-//     the scatter kernel's shared-memory attribute; make that first call
-//     before any stream capture begins.  Later calls only launch kernels and
-//     queue device-to-device copies on `stream`, and return without waiting.
+//     cudaGetSymbolAddress (which may load this file's device code) and raises
+//     the shared-memory limit of the scatter kernel for all four 4/8-byte
+//     (key, value) width pairs, whatever widths that call sorts; make that
+//     first call before any stream capture begins.  Later calls, of any width
+//     pair, only launch kernels and queue device-to-device copies on
+//     `stream`, and return without waiting.
 #include <atomic>
 
 #include "gx_groupby.h"
@@ -36,22 +38,25 @@ namespace gx {
 namespace {
 
 constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(8) << 20;
-constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-std::atomic<void*> g_scratch_addr[NOALLOC_MAX_DEVICES];
+// Device address of g_noalloc_scratch per device ordinal (dev() rejects
+// ordinals of GX_MAX_DEVICES and above); null until that device's set-up ran.
+std::atomic<void*> g_scratch_addr[GX_MAX_DEVICES];
 
 char* noalloc_scratch() {
-    int d = 0;
-    GX_CUDA(cudaGetDevice(&d));
-    if (d < 0 || d >= NOALLOC_MAX_DEVICES) fail(GX_EUNSUPPORTED, "sort_column_pair_noalloc: device ordinal >= 64");
+    const int d = dev().device;
     void* p = g_scratch_addr[d].load(std::memory_order_acquire);
     if (p == nullptr) {
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr)
+        if (e != cudaSuccess || p == nullptr) {
+            (void)cudaGetLastError();
             fail(GX_ECUDA, std::string("sort_column_pair_noalloc: cudaGetSymbolAddress failed: ") +
                                cudaGetErrorString(e));
+        }
+        // Every width pair's scatter attribute now, so no later call changes one.
+        radix_prepare_pair_scatters();
         g_scratch_addr[d].store(p, std::memory_order_release);
     }
     return static_cast<char*>(p);

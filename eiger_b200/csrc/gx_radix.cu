@@ -194,18 +194,24 @@ size_t scatter_smem(int kw, int vw) {
     return (size_t)RS_WARPS * RS_BINS * 4 + RS_BINS * 8 + (RS_BINS + 4) * 4 + (size_t)RS_TILE * (kw + vw);
 }
 
+// The scatter needs more than the default 48 KB of dynamic shared memory,
+// so each instantiation's limit is raised once per device before its first
+// launch.
+template <int KW, int VW, bool IOTA>
+void prepare_scatter() {
+    static per_device_flag attr;
+    attr.once([] {
+        GX_CUDA(cudaFuncSetAttribute(k_radix_scatter<KW, VW, IOTA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)scatter_smem(KW, VW)));
+    });
+}
+
 template <int KW, int VW, bool IOTA>
 void launch_scatter(int64_t ntiles, cudaStream_t s, const void* kin, const void* vin, int64_t n,
                     const img_params& ip, int shift, int dbits, const int64_t* off, void* kout,
                     void* vout) {
     size_t smem = scatter_smem(KW, VW);
-    static bool attr_set[16] = {};
-    int d = dev().device;
-    if (!attr_set[d]) {
-        GX_CUDA(cudaFuncSetAttribute(k_radix_scatter<KW, VW, IOTA>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set[d] = true;
-    }
+    prepare_scatter<KW, VW, IOTA>();
     k_radix_scatter<KW, VW, IOTA><<<(unsigned)ntiles, RS_NT, smem, s>>>(kin, vin, n, ip, shift, dbits,
                                                                        ntiles, off, kout, vout);
     GX_LAUNCHED();
@@ -399,6 +405,16 @@ size_t radix_pairs_scratch_bytes(int64_t n, int key_width, int val_width) {
     size_t b = r256((size_t)n * key_width) + r256((size_t)n * val_width);
     b += r256((size_t)RS_BINS * ntiles * 8) + r256((size_t)RS_BINS * ntiles * 8 + 8);
     return b + scan_scratch_bytes((int64_t)RS_BINS * ntiles);
+}
+
+// Raises the dynamic shared-memory limit of every 4/8-byte (key, value)
+// scatter instantiation on the current device, so later pair sorts of any
+// width combination launch without changing a kernel attribute.
+void radix_prepare_pair_scatters() {
+    prepare_scatter<4, 4, false>();
+    prepare_scatter<4, 8, false>();
+    prepare_scatter<8, 4, false>();
+    prepare_scatter<8, 8, false>();
 }
 
 // The pass loop of radix_sort_biased (bias 0) for 4/8-byte keys and values,

@@ -57,21 +57,23 @@ void prof_read(const char* name, double* total_ms, int64_t* count, bool reset) {
 
 namespace {
 std::mutex g_dev_mu;
-device_info g_dev[16];
-bool g_dev_ok[16] = {};
+device_info g_dev[GX_MAX_DEVICES];
+bool g_dev_ok[GX_MAX_DEVICES] = {};
 
 std::atomic<int64_t> g_cur{0}, g_peak{0};
 std::mutex g_size_mu;
 // Allocation sizes for the stats; the pool itself is CUDA's.
 struct size_rec { void* p; size_t n; };
 std::vector<size_rec> g_sizes;
-bool g_pool_ready[16] = {};
+per_device_flag g_pool_ready;
 }  // namespace
 
 const device_info& dev() {
     int d = 0;
     GX_CUDA(cudaGetDevice(&d));
-    if (d < 0 || d >= 16) d = 0;
+    if (d < 0 || d >= GX_MAX_DEVICES)
+        fail(GX_EUNSUPPORTED, "device ordinal " + std::to_string(d) + " is beyond the " +
+                                  std::to_string(GX_MAX_DEVICES) + " devices this library supports");
     std::lock_guard<std::mutex> g(g_dev_mu);
     if (!g_dev_ok[d]) {
         device_info i;
@@ -86,14 +88,12 @@ const device_info& dev() {
 }
 
 void* pool_alloc(size_t bytes, cudaStream_t s) {
-    int d = dev().device;
-    if (!g_pool_ready[d]) {
+    g_pool_ready.once([] {
         cudaMemPool_t pool;
-        GX_CUDA(cudaDeviceGetDefaultMemPool(&pool, d));
+        GX_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev().device));
         uint64_t thr = UINT64_MAX;
         GX_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-        g_pool_ready[d] = true;
-    }
+    });
     // 256-byte granularity like the reference's slab (mem_manager.cu:102-128).
     size_t rounded = (bytes + 255) & ~size_t(255);
     void* p = nullptr;

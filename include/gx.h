@@ -323,8 +323,10 @@ gx_status gx_argsort(gx_column_view col, int32_t begin_bit, int32_t end_bit, int
  * All calls on a device share the array, so calls that overlap on the
  * device race; order them on one stream or with events.  The first call on
  * a device looks up the array's address (cudaGetSymbolAddress, which may
- * load device code) and sets a kernel attribute: make it before any stream
- * capture begins.  Returns without waiting for the sort to finish. */
+ * load device code) and sets the scatter kernel's shared-memory attribute
+ * for every 4/8-byte width pair: make it before any stream capture begins.
+ * Later calls, of any width pair, only launch kernels and queue copies.
+ * Returns without waiting for the sort to finish. */
 gx_status gx_sort_column_pair_noalloc(gx_column_view key, gx_column_view val, int32_t begin_bit,
                                       int32_t end_bit, int32_t order, void* key_out,
                                       void* val_out, gx_stream_t stream);

@@ -121,3 +121,16 @@ def test_rejects_narrow_columns_and_overlapping_outputs():
     vo = torch.empty_like(v)
     st = noalloc()(gx.view(k32), gx.view(v), 0, -1, gx.ASCENDING, k32.data_ptr(), vo.data_ptr(), None)
     assert st == 1 and "overlap" in gx.last_error()
+
+
+def test_later_calls_of_other_width_pairs_after_the_first():
+    """The first call (4+4 bytes) prepares every width pair; calls of the
+    other three pairs that follow give the allocating sort's result."""
+    import torch
+    for kdt, vdt in ((np.int32, np.int32), (np.int64, np.int64), (np.uint32, np.float64), (np.float64, np.uint32)):
+        k, v = make(123_457, kdt, vdt, 99)
+        ek, ev = gx.sort_column_pair(k, v, 0, -1, gx.ASCENDING)
+        torch.cuda.synchronize()
+        gk, gv = run_noalloc(k, v, 0, -1, gx.ASCENDING)
+        assert torch.equal(gk.view(torch.uint8), ek.view(torch.uint8))
+        assert torch.equal(gv.view(torch.uint8), ev.view(torch.uint8))
