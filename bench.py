@@ -193,6 +193,7 @@ def run_gx(args) -> None:
 
     res = step()
     ngroups = res.num_rows
+    step_result = res.numpy_columns()  # checked against the oracle after timing
     del res
     launches0 = gx.kernel_launches()
     gx.lib.gx_profile_reset()
@@ -260,6 +261,15 @@ def run_gx(args) -> None:
     e2e_ms = time_steps(torch, e2e_step, e2e_steps, 1, dist) / e2e_steps
     e2e = {"value": world * rows / (e2e_ms * 1e-3) / 1e6, "unit": "Mrows/s", "h2d_bytes_per_step": in_bytes,
            "d2h_bytes_per_step": out_bytes, "ms_per_step": e2e_ms}
+    # ------------------------------------------- oracle check + CPU baseline
+    # The oracle (CPU restatement, all host threads) on the same host copies
+    # of the timed workload: it checks the step's output column by column and
+    # its time is the CPU baseline on the full workload.
+    parity, cpu = None, None
+    if rank == 0 and not args.no_check:
+        parity, cpu = check_against_oracle(step_result, hk.numpy(), hiv.numpy(), hfv.numpy())
+        if world > 1:
+            cpu = None  # CPU baseline on single-GPU runs only
     del hk, hiv, hfv
     torch.cuda.empty_cache()
 
@@ -311,7 +321,18 @@ def run_gx(args) -> None:
         zpk = bk[zr.long()]
         del zr, cdf
         join["zipf_1.0"] = measure(lambda: gx.inner_eq_join_rowids(bk, zpk, jh), lambda m: (nb + npr) * 4 + m * 16)
-        del bk, brow, pk, prow, zpk
+        del zpk
+        # The sorted-build matcher: the same join with keys spread 8 apart, so
+        # the build side is too sparse for direct placement; sorted build run
+        # + radix directory (SORTED_BUILD) and both sides sorted (SORT_MERGE).
+        sbk, spk = bk * 8, pk * 8
+        for mode, nm in ((gx.SORTED_BUILD, "sorted_build"), (gx.SORT_MERGE, "sort_merge")):
+            h2 = gx.make_join_hint(gx.JOIN_SORT, gx.MAT_GFUR, unique_left=1, sort_mode=mode)
+            join[nm] = measure(lambda: gx.inner_eq_join_rowids(sbk, spk, h2), lambda m: (nb + npr) * 4 + m * 16)
+        del sbk, spk
+        if rank == 0 and world == 1 and not args.no_cpu:
+            join["cpu_baseline"] = cpu_join_baseline(bk.cpu().numpy(), pk.cpu().numpy())
+        del bk, brow, pk, prow
 
     # ----------------------------------------------------------- batched
     batched = None
@@ -345,8 +366,7 @@ def run_gx(args) -> None:
         torch.cuda.empty_cache()
 
     # ------------------------------------------------------ cpu baseline
-    cpu = None  # timed on rank 0 of single-GPU runs only
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if cpu is None and rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_groupby_baseline(args.cpu_rows, G)
 
     if rank == 0:
@@ -361,7 +381,7 @@ def run_gx(args) -> None:
                        "variant_run": algo_name, "radix_bits": chosen.get("radix_bits"),
                        "selector": "learned" if learned else ("plain" if args.algo == "auto" else "forced"),
                        "l2": "inputs (5.4 GB) larger than L2; no flush"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk.summary(), "join": join, "batched": batched,
         }
         print(json.dumps(line), flush=True)
@@ -443,6 +463,58 @@ def run_join_only(args) -> None:
                       "ms_per_step": ms, "value": (nb + npr) / (ms * 1e-3) / 1e6, "unit": "Mrows/s"}), flush=True)
 
 
+def check_against_oracle(got_cols, k, iv, fv):
+    """Compares the timed step's output with the oracle run on the same
+    input bytes (keys, counts and integer / MIN / MAX columns bit-exact,
+    float64 SUM within 1e-12 relative); the oracle's time on all host threads
+    is the CPU baseline on the full workload."""
+    import oracle as O
+    reqs = [(0, O.SUM), (0, O.MIN), (0, O.MAX), (1, O.SUM), (1, O.MIN), (1, O.MAX), (0, O.COUNT_ALL)]
+    t0 = time.perf_counter()
+    exp = O.groupby(k, [iv, fv], reqs)
+    dt = time.perf_counter() - t0
+    order = np.argsort(got_cols[0], kind="stable")
+    got = [c[order] for c in got_cols]
+    exact, rel = True, 0.0
+    for i, (g, e) in enumerate(zip(got, exp)):
+        if g.shape != e.shape or g.dtype != e.dtype:
+            exact = False
+            continue
+        if i == 4:  # float64 SUM
+            rel = float(np.max(np.abs(g - e) / np.maximum(np.abs(e), 1e-300))) if len(e) else 0.0
+        elif not np.array_equal(g, e):
+            exact = False
+    ok = exact and rel <= 1e-12
+    parity = {"ok": ok, "rows": int(k.shape[0]), "groups": int(len(exp[0])), "exact_columns_equal": exact,
+              "float64_sum_max_rel_err": rel, "tolerance": 1e-12,
+              "check": "step output vs oracle on the same inputs, sorted by key"}
+    cpu = {"value": k.shape[0] / dt / 1e6, "unit": "Mrows/s", "cores": O.num_threads(), "kind": "port",
+           "sample": f"the full workload ({k.shape[0]} rows): radix-partitioned open-addressing group-by, "
+                     "sorted output", "cpu_model": cpu_model()}
+    return parity, cpu
+
+
+def cpu_model() -> str:
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_join_baseline(bk, pk) -> dict:
+    """Parallel CPU hash join (oracle) of the rowid join on the same keys."""
+    import oracle as O
+    t0 = time.perf_counter()
+    l, r = O.join_pairs_parallel(bk, pk)
+    dt = time.perf_counter() - t0
+    return {"value": (len(bk) + len(pk)) / dt / 1e6, "unit": "Mrows/s", "cores": O.num_threads(), "kind": "port",
+            "matches": int(len(l)), "sample": "the full join (chained hash build, parallel probe, pairs written)",
+            "cpu_model": cpu_model()}
+
+
 def cpu_groupby_baseline(rows: int, groups: int) -> dict:
     """The oracle (CPU restatement, all host threads) on a bounded sample."""
     import oracle as O
@@ -485,7 +557,7 @@ def run_reference(args) -> None:
                        "rows": args.rows, "groups": G, "sample_rows": rows},
             "cpu_baseline": {"value": value, "unit": "Mrows/s", "cores": O.num_threads(), "kind": "port",
                              "sample": f"{rows} rows per step (the reference has no CPU operators; this is "
-                                       "the CPU restatement of its group-by)"},
+                                       "the CPU restatement of its group-by)", "cpu_model": cpu_model()},
             "e2e": {"value": value, "unit": "Mrows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -507,6 +579,7 @@ def main() -> None:
                     help="AUTO's chooser: the learned FP16 MLP (committed weights) or the plain NDV rule")
     ap.add_argument("--batch-instances", type=int, default=512, help="batched pipeline instances (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-check", action="store_true", help="skip the oracle check of the timed step's output")
     ap.add_argument("--cpu-rows", type=int, default=1 << 24)
     ap.add_argument("--traffic", type=float, default=None,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")

@@ -31,7 +31,7 @@ def build() -> Path:
     if LIB.exists() and LIB.stat().st_mtime >= SRC.stat().st_mtime:
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", str(SRC), "-o", str(tmp)]
+    cmd = ["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", str(SRC), "-o", str(tmp)]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB
@@ -55,6 +55,10 @@ def lib() -> C.CDLL:
         L.orc_join_pairs.restype = i64
         L.orc_join_count_parallel.argtypes = [vp, i64, vp, i64, i32]
         L.orc_join_count_parallel.restype = i64
+        L.orc_join_probe_unique.argtypes = [vp, i64, vp, i64, i32, vp]
+        L.orc_join_probe_unique.restype = i64
+        L.orc_join_pairs_parallel.argtypes = [vp, i64, vp, i64, i32, vp, vp]
+        L.orc_join_pairs_parallel.restype = i64
         L.orc_dict_encode.argtypes = [vp, i32, i64, i32, vp]
         L.orc_dict_encode.restype = i64
         L.orc_dict_with_dict.argtypes = [vp, i64, vp, i64, i32, vp]
@@ -149,6 +153,30 @@ def join_pairs(lkeys: np.ndarray, rkeys: np.ndarray):
     m = L.orc_join_pairs(_p(lkeys), lkeys.shape[0], _p(rkeys), rkeys.shape[0], t, None, None)
     ol, orr = np.empty(max(m, 1), np.int64), np.empty(max(m, 1), np.int64)
     L.orc_join_pairs(_p(lkeys), lkeys.shape[0], _p(rkeys), rkeys.shape[0], t, _p(ol), _p(orr))
+    return ol[:m], orr[:m]
+
+
+def join_probe_unique(lkeys: np.ndarray, rkeys: np.ndarray) -> np.ndarray:
+    """For a left side with unique keys: match[j] = left row equal to right
+    row j, or -1.  The join's pairs are (match[j], j) where match[j] >= 0."""
+    lkeys, rkeys = np.ascontiguousarray(lkeys), np.ascontiguousarray(rkeys)
+    match = np.empty(rkeys.shape[0], dtype=np.int64)
+    rc = lib().orc_join_probe_unique(_p(lkeys), lkeys.shape[0], _p(rkeys), rkeys.shape[0], gx_type(lkeys),
+                                     _p(match))
+    if rc != 0:
+        raise ValueError("join_probe_unique: left keys are not unique")
+    return match
+
+
+def join_pairs_parallel(lkeys: np.ndarray, rkeys: np.ndarray):
+    """All (left_row, right_row) pairs with equal keys in right-row order
+    (the parallel CPU join baseline; sort them for the canonical order)."""
+    L = lib()
+    lkeys, rkeys = np.ascontiguousarray(lkeys), np.ascontiguousarray(rkeys)
+    t = gx_type(lkeys)
+    m = L.orc_join_pairs_parallel(_p(lkeys), lkeys.shape[0], _p(rkeys), rkeys.shape[0], t, None, None)
+    ol, orr = np.empty(max(m, 1), np.int64), np.empty(max(m, 1), np.int64)
+    L.orc_join_pairs_parallel(_p(lkeys), lkeys.shape[0], _p(rkeys), rkeys.shape[0], t, _p(ol), _p(orr))
     return ol[:m], orr[:m]
 
 

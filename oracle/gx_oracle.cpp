@@ -30,8 +30,8 @@
 //   * dictionary encodings: compress/dictionary_encode.cu:71-142,
 //     compress/dictionary_encode_dict_ready.cu:35-58 (absent value -> INT32_MIN).
 // Group-by results are returned sorted by key (canonical order); float SUM
-// accumulates in long double so the oracle is closer to the exact sum than
-// any device summation order.
+// accumulates in long double, in row order, so the oracle is closer to the
+// exact sum than any device summation order.
 #include <omp.h>
 #include <stdint.h>
 #include <string.h>
@@ -40,6 +40,7 @@
 #include <cmath>
 #include <limits>
 #include <numeric>
+#include <parallel/algorithm>
 #include <unordered_map>
 #include <vector>
 
@@ -114,53 +115,59 @@ int64_t as_i64(const void* p, int t, int64_t i) {
     }
 }
 
-// Per-group accumulator: integer sums wrap in uint64, floats in long double.
-struct acc {
-    uint64_t isum = 0;
-    long double fsum = 0;
-    long double fmin = 0, fmax = 0;
-    int64_t smin = 0, smax = 0;
-    uint64_t umin = 0, umax = 0;
-    uint64_t any = 0;
-    bool seen = false;  // min/max initialised (a NaN-only group keeps identities)
+// Per-group accumulator of one value column: integer sums wrap in uint64,
+// float sums accumulate in long double; mn / mx hold the extreme's bits
+// (int64 / uint64 value, or the double for float columns); NaN does not take
+// part in MIN / MAX, and a group with no non-NaN value keeps seen = false.
+struct cacc {
+    long double fsum;
+    uint64_t isum;
+    uint64_t mn, mx;
+    uint64_t any;
+    bool seen;
 };
 
-struct group {
-    uint64_t key_raw;
-    int64_t count = 0;
-    std::vector<acc> a;
-};
+void cacc_init(cacc& x, uint64_t any_bits) {
+    x.fsum = 0;
+    x.isum = 0;
+    x.mn = x.mx = 0;
+    x.any = any_bits;
+    x.seen = false;
+}
 
-void update(acc& x, int kind, const void* col, int t, int64_t i) {
+void cacc_update(cacc& x, const void* col, int t, int64_t i) {
     if (is_f(t)) {
-        long double v = as_ld(col, t, i);
-        x.fsum += v;
-        if (!std::isnan((double)v)) {
-            if (!x.seen) { x.fmin = x.fmax = v; x.seen = true; }
-            else { if (v < x.fmin) x.fmin = v; if (v > x.fmax) x.fmax = v; }
-        }
+        const double v = t == T_F32 ? (double)((const float*)col)[i] : ((const double*)col)[i];
+        x.fsum += (long double)v;
+        if (std::isnan(v)) return;
+        uint64_t b;
+        memcpy(&b, &v, 8);
+        if (!x.seen) { x.mn = x.mx = b; x.seen = true; return; }
+        double mn, mx;
+        memcpy(&mn, &x.mn, 8);
+        memcpy(&mx, &x.mx, 8);
+        if (v < mn) x.mn = b;
+        if (v > mx) x.mx = b;
     } else if (is_s(t)) {
-        int64_t v = as_i64(col, t, i);
+        const int64_t v = as_i64(col, t, i);
         x.isum += (uint64_t)v;
-        if (!x.seen) { x.smin = x.smax = v; x.seen = true; }
-        else { x.smin = std::min(x.smin, v); x.smax = std::max(x.smax, v); }
+        if (!x.seen) { x.mn = x.mx = (uint64_t)v; x.seen = true; return; }
+        if (v < (int64_t)x.mn) x.mn = (uint64_t)v;
+        if (v > (int64_t)x.mx) x.mx = (uint64_t)v;
     } else {
-        uint64_t v = raw_bits(col, t, i);
+        const uint64_t v = raw_bits(col, t, i);
         x.isum += v;
-        if (!x.seen) { x.umin = x.umax = v; x.seen = true; }
-        else { x.umin = std::min(x.umin, v); x.umax = std::max(x.umax, v); }
+        if (!x.seen) { x.mn = x.mx = v; x.seen = true; return; }
+        if (v < x.mn) x.mn = v;
+        if (v > x.mx) x.mx = v;
     }
-    (void)kind;
 }
-void merge(acc& x, const acc& y, int t) {
-    x.isum += y.isum;
-    x.fsum += y.fsum;
-    if (!y.seen) return;
-    if (!x.seen) { long double s = x.fsum; uint64_t is = x.isum; uint64_t an = x.any; x = y; x.fsum = s; x.isum = is; x.any = an; return; }
-    if (is_f(t)) { x.fmin = std::min(x.fmin, y.fmin); x.fmax = std::max(x.fmax, y.fmax); }
-    else if (is_s(t)) { x.smin = std::min(x.smin, y.smin); x.smax = std::max(x.smax, y.smax); }
-    else { x.umin = std::min(x.umin, y.umin); x.umax = std::max(x.umax, y.umax); }
+
+uint64_t o_fmix64(uint64_t x) {
+    x ^= x >> 33; x *= 0xff51afd7ed558ccdULL; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ULL; x ^= x >> 33;
+    return x;
 }
+int ceil_log2(uint64_t x) { int b = 0; while ((1ull << b) < x) ++b; return b; }
 
 int out_type(int kind, int t) {
     if (kind == A_COUNT) return T_I64;
@@ -198,73 +205,140 @@ void orc_set_threads(int n) { if (n > 0) omp_set_num_threads(n); }
 // outputs: out_key (capacity n, key type), out[r] (capacity n, output type of
 // request r; when agg_count an extra trailing int64 count column).
 // Returns the number of groups, sorted ascending by key.
+//
+// Method (also the timed CPU baseline): radix-partition the row ids by the
+// top bits of a 64-bit key hash (per-thread counts, prefix, stable scatter, so
+// each partition keeps row order), then aggregate every partition with its
+// own open-addressing table, partitions spread over the threads.  Partitions
+// hold disjoint keys, so nothing is merged; each group sees its rows in row
+// order, which fixes ANY (first row) and the long double float sums.
 // ---------------------------------------------------------------------------
 int64_t orc_groupby(const void* keys, int key_type, int64_t n, int nvals, const void* const* vals,
                     const int* val_types, int nreq, const int64_t* req_cols, const int* req_kinds,
                     int agg_count, void* out_key, void* const* out) {
-    const int nthreads = omp_get_max_threads();
-    std::vector<std::unordered_map<uint64_t, int64_t>> maps(nthreads);
-    std::vector<std::vector<group>> groups(nthreads);
-#pragma omp parallel num_threads(nthreads)
+    if ((uint64_t)n >= (1ull << 32)) return -1;
+    const int T = omp_get_max_threads();
+    int pb = 0;
+    if (n >= (1 << 16)) pb = std::min(12, ceil_log2((uint64_t)n >> 15));
+    const int64_t P = int64_t(1) << pb;
+    auto khash = [&](uint64_t k) { return o_fmix64(k ^ 0x9E3779B97F4A7C15ull); };
+    auto part_of = [&](int64_t i) -> int64_t {
+        return pb ? (int64_t)(khash(canon(raw_bits(keys, key_type, i), key_type)) >> (64 - pb)) : 0;
+    };
+    std::vector<int64_t> cnt((size_t)T * P, 0), off((size_t)T * P, 0), start(P + 1, 0);
+#pragma omp parallel num_threads(T)
     {
-        int t = omp_get_thread_num();
-        auto& m = maps[t];
-        auto& gs = groups[t];
-        int64_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
-        for (int64_t i = lo; i < hi; ++i) {
-            uint64_t raw = raw_bits(keys, key_type, i);
-            uint64_t k = canon(raw, key_type);
-            auto it = m.find(k);
-            int64_t g;
-            if (it == m.end()) {
-                g = (int64_t)gs.size();
-                m.emplace(k, g);
-                group ng;
-                ng.key_raw = raw;
-                ng.a.resize(nvals);
-                for (int c = 0; c < nvals; ++c) ng.a[c].any = raw_bits(vals[c], val_types[c], i);
-                gs.push_back(std::move(ng));
-            } else {
-                g = it->second;
-            }
-            group& G = gs[g];
-            G.count++;
-            for (int c = 0; c < nvals; ++c) update(G.a[c], 0, vals[c], val_types[c], i);
-        }
+        const int t = omp_get_thread_num();
+        const int64_t lo = n * t / T, hi = n * (t + 1) / T;
+        int64_t* c = &cnt[(size_t)t * P];
+        for (int64_t i = lo; i < hi; ++i) c[part_of(i)]++;
     }
-    // Merge per-thread groups in thread order (deterministic).
-    std::unordered_map<uint64_t, int64_t> all;
-    std::vector<group> merged;
-    for (int t = 0; t < nthreads; ++t) {
-        for (auto& g : groups[t]) {
-            uint64_t k = canon(g.key_raw, key_type);
-            auto it = all.find(k);
-            if (it == all.end()) {
-                all.emplace(k, (int64_t)merged.size());
-                merged.push_back(std::move(g));
-            } else {
-                group& M = merged[it->second];
-                M.count += g.count;
-                for (int c = 0; c < nvals; ++c) merge(M.a[c], g.a[c], val_types[c]);
-            }
-        }
+    int64_t run = 0;
+    for (int64_t p = 0; p < P; ++p) {
+        start[p] = run;
+        for (int t = 0; t < T; ++t) { off[(size_t)t * P + p] = run; run += cnt[(size_t)t * P + p]; }
     }
-    std::vector<int64_t> order(merged.size());
-    std::iota(order.begin(), order.end(), 0);
-    std::sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
-        return image(canon(merged[x].key_raw, key_type), key_type) < image(canon(merged[y].key_raw, key_type), key_type);
-    });
+    start[P] = run;
+    std::vector<uint32_t> idx((size_t)n);
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num();
+        const int64_t lo = n * t / T, hi = n * (t + 1) / T;
+        int64_t* o = &off[(size_t)t * P];
+        for (int64_t i = lo; i < hi; ++i) idx[(size_t)o[part_of(i)]++] = (uint32_t)i;
+    }
+    struct part_out {
+        std::vector<uint64_t> key_raw;
+        std::vector<int64_t> count;
+        std::vector<cacc> a;  // nvals per group
+    };
+    std::vector<part_out> po((size_t)P);
+    // Per-thread working table and group lists, reused from partition to
+    // partition (growing vectors per partition costs fresh pages and unmaps
+    // on every growth step); each partition's groups are copied out once.
+    std::vector<part_out> work((size_t)T);
+    std::vector<std::vector<uint64_t>> wtk((size_t)T);
+    std::vector<std::vector<int32_t>> wtg((size_t)T);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(T)
+    for (int64_t p = 0; p < P; ++p) {
+        const int t = omp_get_thread_num();
+        part_out& o = work[(size_t)t];
+        std::vector<uint64_t>& tk = wtk[(size_t)t];
+        std::vector<int32_t>& tg = wtg[(size_t)t];
+        o.key_raw.clear();
+        o.count.clear();
+        o.a.clear();
+        uint64_t cap = 1024;
+        if (tk.size() < cap) { tk.resize(cap); tg.resize(cap); }
+        std::fill(tg.begin(), tg.begin() + (int64_t)cap, -1);
+        for (int64_t j = start[p]; j < start[p + 1]; ++j) {
+            const int64_t i = idx[(size_t)j];
+            const uint64_t raw = raw_bits(keys, key_type, i), k = canon(raw, key_type);
+            uint64_t slot = khash(k) & (cap - 1);
+            int32_t g;
+            for (;;) {
+                if (tg[slot] < 0) {
+                    g = (int32_t)o.count.size();
+                    tg[slot] = g;
+                    tk[slot] = k;
+                    o.key_raw.push_back(raw);
+                    o.count.push_back(0);
+                    for (int c = 0; c < nvals; ++c) {
+                        cacc x;
+                        cacc_init(x, raw_bits(vals[c], val_types[c], i));
+                        o.a.push_back(x);
+                    }
+                    if ((uint64_t)o.count.size() * 2 > cap) {  // keep load <= 1/2: rebuild at twice the size
+                        cap *= 2;
+                        if (tk.size() < cap) { tk.resize(cap); tg.resize(cap); }
+                        std::fill(tg.begin(), tg.begin() + (int64_t)cap, -1);
+                        for (size_t q = 0; q < o.count.size(); ++q) {
+                            const uint64_t kq = canon(o.key_raw[q], key_type);
+                            uint64_t sq = khash(kq) & (cap - 1);
+                            while (tg[sq] >= 0) sq = (sq + 1) & (cap - 1);
+                            tg[sq] = (int32_t)q;
+                            tk[sq] = kq;
+                        }
+                    }
+                    break;
+                }
+                if (tk[slot] == k) { g = tg[slot]; break; }
+                slot = (slot + 1) & (cap - 1);
+            }
+            o.count[(size_t)g]++;
+            for (int c = 0; c < nvals; ++c) cacc_update(o.a[(size_t)g * nvals + c], vals[c], val_types[c], i);
+        }
+        part_out& dst = po[(size_t)p];
+        dst.key_raw.assign(o.key_raw.begin(), o.key_raw.end());
+        dst.count.assign(o.count.begin(), o.count.end());
+        dst.a.assign(o.a.begin(), o.a.end());
+    }
+    // Canonical order: ascending key image.
+    struct gref { uint64_t img; uint32_t p, g; };
+    std::vector<int64_t> gstart(P + 1, 0);
+    for (int64_t p = 0; p < P; ++p) gstart[p + 1] = gstart[p] + (int64_t)po[(size_t)p].count.size();
+    const int64_t G = gstart[P];
+    std::vector<gref> order((size_t)G);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(T)
+    for (int64_t p = 0; p < P; ++p)
+        for (size_t g = 0; g < po[(size_t)p].count.size(); ++g)
+            order[(size_t)(gstart[p] + (int64_t)g)] = {image(canon(po[(size_t)p].key_raw[g], key_type), key_type),
+                                                       (uint32_t)p, (uint32_t)g};
+    __gnu_parallel::sort(order.begin(), order.end(), [](const gref& x, const gref& y) { return x.img < y.img; });
     const int kw = width(key_type);
-    for (size_t gi = 0; gi < order.size(); ++gi) {
-        const group& G = merged[order[gi]];
-        memcpy((char*)out_key + gi * kw, &G.key_raw, kw);
+#pragma omp parallel for schedule(static) num_threads(T)
+    for (int64_t gi = 0; gi < G; ++gi) {
+        const part_out& o = po[order[(size_t)gi].p];
+        const size_t g = order[(size_t)gi].g;
+        const int64_t count = o.count[g];
+        memcpy((char*)out_key + gi * kw, &o.key_raw[g], kw);
         for (int r = 0; r < nreq; ++r) {
-            int kind = req_kinds[r];
-            if (kind == A_COUNT) { ((int64_t*)out[r])[gi] = G.count; continue; }
-            int c = (int)req_cols[r];
-            int t = val_types[c];
-            const acc& x = G.a[c];
-            int ot = out_type(kind, t);
+            const int kind = req_kinds[r];
+            if (kind == A_COUNT) { ((int64_t*)out[r])[gi] = count; continue; }
+            const int c = (int)req_cols[r];
+            const int t = val_types[c];
+            const cacc& x = o.a[g * nvals + c];
+            const int ot = out_type(kind, t);
             switch (kind) {
                 case A_SUM:
                     if (is_f(t)) store(out[r], ot, gi, 0, x.fsum, true);
@@ -272,14 +346,18 @@ int64_t orc_groupby(const void* keys, int key_type, int64_t n, int nvals, const 
                     break;
                 case A_AVG: {
                     long double num = is_f(t) ? x.fsum : (is_s(t) ? (long double)(int64_t)x.isum : (long double)x.isum);
-                    ((double*)out[r])[gi] = (double)(num / (long double)G.count);
+                    ((double*)out[r])[gi] = (double)(num / (long double)count);
                     break;
                 }
                 case A_MIN: case A_MAX: {
-                    bool mn = kind == A_MIN;
-                    if (is_f(t)) store(out[r], ot, gi, 0, mn ? x.fmin : x.fmax, true);
-                    else if (is_s(t)) store(out[r], ot, gi, (uint64_t)(mn ? x.smin : x.smax), 0, false);
-                    else store(out[r], ot, gi, mn ? x.umin : x.umax, 0, false);
+                    const uint64_t b = kind == A_MIN ? x.mn : x.mx;
+                    if (is_f(t)) {
+                        double d = 0;
+                        if (x.seen) memcpy(&d, &b, 8);
+                        store(out[r], ot, gi, 0, (long double)d, true);
+                    } else {
+                        store(out[r], ot, gi, x.seen ? b : 0, 0, false);
+                    }
                     break;
                 }
                 case A_ANY: {
@@ -289,9 +367,9 @@ int64_t orc_groupby(const void* keys, int key_type, int64_t n, int nvals, const 
                 }
             }
         }
-        if (agg_count) ((int64_t*)out[nreq])[gi] = G.count;
+        if (agg_count) ((int64_t*)out[nreq])[gi] = count;
     }
-    return (int64_t)order.size();
+    return G;
 }
 
 // ---------------------------------------------------------------------------
@@ -375,6 +453,82 @@ int64_t orc_join_count_parallel(const void* lkeys, int64_t nl, const void* rkeys
     return total;
 }
 
+// Unique-build probe: match[j] = the left row whose key equals right row j's,
+// or -1.  Returns 0, or -1 when the left keys are not unique (match is then
+// unspecified).  Every (left, right) pair of the join is (match[j], j) for
+// match[j] >= 0, so this checks a join of a unique build side in O(n).
+int64_t orc_join_probe_unique(const void* lkeys, int64_t nl, const void* rkeys, int64_t nr, int key_type,
+                              int64_t* match) {
+    const uint64_t cap = 1ull << ceil_log2((uint64_t)std::max<int64_t>(2 * nl, 2));
+    std::vector<uint64_t> tk(cap);
+    std::vector<int64_t> tr(cap, -1);
+    for (int64_t i = 0; i < nl; ++i) {
+        const uint64_t k = canon(raw_bits(lkeys, key_type, i), key_type);
+        uint64_t s = o_fmix64(k) & (cap - 1);
+        while (tr[s] >= 0) {
+            if (tk[s] == k) return -1;
+            s = (s + 1) & (cap - 1);
+        }
+        tk[s] = k;
+        tr[s] = i;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < nr; ++j) {
+        const uint64_t k = canon(raw_bits(rkeys, key_type, j), key_type);
+        uint64_t s = o_fmix64(k) & (cap - 1);
+        int64_t m = -1;
+        while (tr[s] >= 0) {
+            if (tk[s] == k) { m = tr[s]; break; }
+            s = (s + 1) & (cap - 1);
+        }
+        match[j] = m;
+    }
+    return 0;
+}
+
+// Parallel hash join (the timed CPU join baseline): chained table over the
+// left keys, right rows probed by all threads; pairs are written in right-row
+// order, each right row's matches in descending left row order.  Call with
+// out_l == null for the count only.
+int64_t orc_join_pairs_parallel(const void* lkeys, int64_t nl, const void* rkeys, int64_t nr, int key_type,
+                                int64_t* out_l, int64_t* out_r) {
+    const uint64_t cap = 1ull << ceil_log2((uint64_t)std::max<int64_t>(nl, 2));
+    std::vector<int64_t> head(cap, -1), next((size_t)std::max<int64_t>(nl, 1));
+    std::vector<uint64_t> lk((size_t)std::max<int64_t>(nl, 1));
+    for (int64_t i = 0; i < nl; ++i) {
+        const uint64_t k = canon(raw_bits(lkeys, key_type, i), key_type);
+        const uint64_t s = o_fmix64(k) & (cap - 1);
+        lk[i] = k;
+        next[i] = head[s];
+        head[s] = i;
+    }
+    const int T = omp_get_max_threads();
+    std::vector<int64_t> part(T + 1, 0);
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num();
+        const int64_t lo = nr * t / T, hi = nr * (t + 1) / T;
+        int64_t c = 0;
+        for (int64_t j = lo; j < hi; ++j) {
+            const uint64_t k = canon(raw_bits(rkeys, key_type, j), key_type);
+            for (int64_t i = head[o_fmix64(k) & (cap - 1)]; i >= 0; i = next[i]) c += lk[i] == k;
+        }
+        part[t + 1] = c;
+#pragma omp barrier
+#pragma omp single
+        for (int q = 0; q < T; ++q) part[q + 1] += part[q];
+        if (out_l) {
+            int64_t w = part[t];
+            for (int64_t j = lo; j < hi; ++j) {
+                const uint64_t k = canon(raw_bits(rkeys, key_type, j), key_type);
+                for (int64_t i = head[o_fmix64(k) & (cap - 1)]; i >= 0; i = next[i])
+                    if (lk[i] == k) { out_l[w] = i; out_r[w] = j; ++w; }
+            }
+        }
+    }
+    return part[T];
+}
+
 // ---------------------------------------------------------------------------
 // Dictionary encoding.  mode 0: codes in first-occurrence order; mode 1:
 // code = rank of the value among distinct values.  Returns NDV.
@@ -426,10 +580,6 @@ int64_t orc_ndv_exact(const void* keys, int key_type, int64_t n) {
 // HyperLogLog (p = 13) restated from Flajolet et al. 2007 with the same hash
 // and register rule as the device sketch, so registers match bit for bit.
 // ---------------------------------------------------------------------------
-static uint64_t o_fmix64(uint64_t x) {
-    x ^= x >> 33; x *= 0xff51afd7ed558ccdULL; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ULL; x ^= x >> 33;
-    return x;
-}
 void orc_hll_registers(const void* keys, int key_type, int64_t n, int64_t stride, uint32_t* regs) {
     const int P = 13;
     memset(regs, 0, sizeof(uint32_t) << P);
@@ -481,7 +631,6 @@ static uint64_t perm_range(uint64_t i, uint64_t n, int k, uint64_t key) {
     do { x = perm_bits(x, k, key); } while (x >= n);
     return x;
 }
-static int ceil_log2(uint64_t x) { int b = 0; while ((1ull << b) < x) ++b; return b; }
 static uint32_t o_fmix32(uint32_t x) {
     x ^= x >> 16; x *= 0x85ebca6bU; x ^= x >> 13; x *= 0xc2b2ae35U; x ^= x >> 16;
     return x;

@@ -6,8 +6,8 @@ form the key and value tables, the aggregation requests, the hint flags, and
 the expected results the test asserts (std::map `expected` literals, the
 per-key if/else EXPECT blocks and single-row EXPECTs).  Nothing is executed.
 
-Run in a checkout that has the reference at REF (default /root/reference):
-    python tests/golden/make_golden.py [REF]
+Run with the path of a checkout of the reference project:
+    python tests/golden/make_golden.py REF
 """
 from __future__ import annotations
 
@@ -16,7 +16,9 @@ import re
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
+REF = Path(sys.argv[1])
 SRC = REF / "src/cuda/tests/groupby/groupby_multikeys_test.cu"
 OUT = Path(__file__).resolve().parent / "groupby_multikeys.json"
 
