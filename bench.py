@@ -322,6 +322,11 @@ def run_gx(args) -> None:
         del zr, cdf
         join["zipf_1.0"] = measure(lambda: gx.inner_eq_join_rowids(bk, zpk, jh), lambda m: (nb + npr) * 4 + m * 16)
         del zpk
+        # The hash multiset (join_algo HASH) and the partitioned hash join
+        # (join_algo PARTITION) on the same keys.
+        for algo, nm in ((gx.JOIN_HASH, "hash"), (gx.JOIN_PARTITION, "partition_hash")):
+            h3 = gx.make_join_hint(algo, gx.MAT_GFUR, unique_left=1)
+            join[nm] = measure(lambda: gx.inner_eq_join_rowids(bk, pk, h3), lambda m: (nb + npr) * 4 + m * 16)
         # The sorted-build matcher: the same join with keys spread 8 apart, so
         # the build side is too sparse for direct placement; sorted build run
         # + radix directory (SORTED_BUILD) and both sides sorted (SORT_MERGE).

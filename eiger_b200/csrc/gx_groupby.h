@@ -35,6 +35,11 @@ void sort_groupby(const col& key, const agg_plan& p, gx_groupby_hint* hint, bool
 void partition_groupby(const col& key, const agg_plan& p, gx_groupby_hint* hint, bool gfur,
                        cudaStream_t s, gx_table* out);
 
+// Radix-partitions (key, row id) by R bits of the partition hash; see
+// gx_groupby_partition.cu.
+void hash_partition_rows(const col& key, int R, void* keys_out, int64_t* rows_out, int64_t* part_start,
+                         cudaStream_t s);
+
 // ----- radix sort / partition (gx_radix.cu) -----
 // Stable LSD radix sort of (key, value) on bits [begin_bit, end_bit) of the
 // order-preserving key image.  vals_in may be null (keys only) or, with

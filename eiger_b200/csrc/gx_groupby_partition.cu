@@ -1050,6 +1050,53 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     fail(GX_EOVERFLOW, "partition group-by spill table overflow after retries");
 }
 
+// Radix-partitions a 4/8-byte key column by R bits of the partition hash
+// (the id PARTITION group-by uses: fmix of the canonical key bits), moving
+// every key with its row id.  keys_out / rows_out hold n entries; partition
+// p is rows [part_start[p], part_start[p + 1]) of them (2^R + 1 starts).
+// Row order inside a partition is unspecified.
+void hash_partition_rows(const col& key, int R, void* keys_out, int64_t* rows_out, int64_t* part_start,
+                         cudaStream_t s) {
+    const int64_t n = key.n;
+    const int kw = size_of(key.type);
+    const int kind = vkind_of(key.type);
+    require(kw == 4 || kw == 8, "hash partition: 4- or 8-byte keys");
+    require(R >= 1 && R <= 16, "hash partition: 1..16 radix bits");
+    const int P = 1 << R;
+    if (n == 0) {
+        fill_u64(part_start, 0, P + 1, s);
+        return;
+    }
+    move_cols mc;
+    std::memset(&mc, 0, sizeof(mc));
+    mc.n = 2;
+    mc.in[0] = key.data; mc.width[0] = kw; mc.out[0] = keys_out;
+    mc.in[1] = nullptr;  mc.width[1] = 8;  mc.iota[1] = 1; mc.out[1] = rows_out;
+    const int64_t ntiles = ceil_div(n, PS_TILE);
+    dbuf counts((size_t)PS_BINS * ntiles * 8, s), offs((size_t)PS_BINS * ntiles * 8 + 8, s), flag(8, s);
+    GX_CUDA(cudaMemsetAsync(flag.get(), 0, 8, s));
+    const int passes = (R + 7) / 8;
+    dbuf tk, tr;
+    if (passes == 2) { tk = dbuf((size_t)n * kw, s); tr = dbuf((size_t)n * 8, s); }
+    int shift = 0;
+    for (int ps = 0; ps < passes; ++ps) {
+        const int dbits = std::min(8, R - shift);
+        move_cols m = mc;
+        if (passes == 2 && ps == 0) { m.out[0] = tk.get(); m.out[1] = tr.get(); }
+        if (passes == 2 && ps == 1) { m.in[0] = tk.get(); m.in[1] = tr.get(); m.iota[1] = 0; }
+        if (kw == 4) part_pass<4>(m.in[0], n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), flag.get<int>(), ps > 0, s);
+        else part_pass<8>(m.in[0], n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), flag.get<int>(), ps > 0, s);
+        shift += dbits;
+    }
+    if (passes == 1) {
+        k_starts_from_offsets<<<(unsigned)ceil_div(P + 1, 256), 256, 0, s>>>(offs.get<int64_t>(), ntiles, P, n, part_start);
+        GX_LAUNCHED();
+    } else {
+        partition_starts(keys_out, kw, n, kind, R, part_start, s);
+    }
+    if (read_scalar(flag.get<int>(), s)) fail(GX_ETIMEOUT, "hash partition: a bulk copy into shared memory did not complete");
+}
+
 namespace {
 template <int KW>
 __global__ void k_part_starts(const void* __restrict__ keys, int64_t n, int kind, int R, int64_t* __restrict__ ps, int P) {

@@ -22,7 +22,7 @@
 // structure, kept for comparison.
 #include <algorithm>
 
-#include "gx_groupby.h"
+#include "gx_join.h"
 
 namespace gx {
 
@@ -35,7 +35,6 @@ namespace {
 constexpr int JP_NT = 256;
 constexpr int JP_IPT = 16;  // 16 rows per thread: 4096-row tiles (measured best of 8/16/32)
 constexpr int JP_TILE = JP_NT * JP_IPT;
-constexpr int MAX_PAY = 8;
 
 template <int KW>
 __device__ __forceinline__ uint64_t img_of(const void* p, int64_t i, int kind) {
@@ -147,38 +146,6 @@ __global__ void __launch_bounds__(JP_NT) k_probe_count(build_run b, probe_side p
         int64_t t = 0;
         for (int j = 0; j < JP_NT / 32; ++j) t += sm[j];
         tile_out[blockIdx.x] = t;
-    }
-}
-
-struct join_out {
-    // Output columns: key, then `n_build_pay` build payloads, then `n_probe_pay`.
-    void* key;              // may be null (row-id form)
-    int key_width;
-    int n_pay;              // total payload outputs
-    void* out[2 * MAX_PAY + 2];
-    int width[2 * MAX_PAY + 2];
-    // source: 0 = build run value (sorted payload / row id), 1 = build column
-    // gathered by build row id, 2 = probe column at probe row, 3 = build row id,
-    // 4 = probe row id
-    int src[2 * MAX_PAY + 2];
-    const void* col[2 * MAX_PAY + 2];
-};
-
-__device__ __forceinline__ uint64_t ld_w(const void* p, int w, int64_t i) {
-    switch (w) {
-        case 8: return __ldg(static_cast<const unsigned long long*>(p) + i);
-        case 4: return __ldg(static_cast<const unsigned*>(p) + i);
-        case 2: return static_cast<const uint16_t*>(p)[i];
-        default: return static_cast<const uint8_t*>(p)[i];
-    }
-}
-// Join outputs are written once: 4/8-byte stores use the streaming hint.
-__device__ __forceinline__ void st_w(void* p, int w, int64_t i, uint64_t v) {
-    switch (w) {
-        case 8: __stcs(static_cast<unsigned long long*>(p) + i, (unsigned long long)v); break;
-        case 4: __stcs(static_cast<unsigned*>(p) + i, (unsigned)v); break;
-        case 2: static_cast<uint16_t*>(p)[i] = (uint16_t)v; break;
-        default: static_cast<uint8_t*>(p)[i] = (uint8_t)v; break;
     }
 }
 
@@ -483,15 +450,10 @@ __global__ void __launch_bounds__(JP_NT) k_dense_probe1(const void* __restrict__
     }
 }
 
-struct join_inputs {
-    col lkey, rkey;
-    std::vector<col> lpay, rpay;
-};
-
 // Output columns of a join: [key, left payloads.., right payloads..] or the
 // row-id pair; `dense` selects the source codes of the dense path.
-static join_out make_outputs(const join_inputs& in, bool build_left, bool rowids_only, bool pay_in_run, bool dense,
-                             int64_t total, cudaStream_t s, gx_table* out, int64_t cap = -1) {
+join_out make_outputs(const join_inputs& in, bool build_left, bool rowids_only, bool pay_in_run, bool dense,
+                      int64_t total, cudaStream_t s, gx_table* out, int64_t cap) {
     join_out o;
     std::memset(&o, 0, sizeof(o));
     out->cols.clear();
@@ -691,6 +653,17 @@ static void join_core(const join_inputs& in, const gx_join_hint& hint, bool rowi
     GX_CUDA(cudaStreamSynchronize(s));
 }
 
+// join_algo picks the plan: SORT (dense placement or sorted build + radix
+// directory, above), HASH (global multiset) or PARTITION (radix-partitioned
+// shared-memory tables), the last two in gx_join_hash.cu.  All three return
+// the same pair multiset.
+static void run_join(const join_inputs& in, const gx_join_hint& hint, bool rowids_only, cudaStream_t s,
+                     gx_table* out) {
+    if (hint.join_algo == GX_JOIN_HASH) hash_join(in, hint, rowids_only, s, out);
+    else if (hint.join_algo == GX_JOIN_PARTITION) partition_hash_join(in, hint, rowids_only, s, out);
+    else join_core(in, hint, rowids_only, s, out);
+}
+
 void inner_eq_join(const gx_table_view* left, const gx_table_view* right, const gx_join_hint* hint,
                    cudaStream_t s, gx_table* out) {
     require(left && right && hint, "join: null argument");
@@ -704,10 +677,6 @@ void inner_eq_join(const gx_table_view* left, const gx_table_view* right, const 
     if (left->columns[0].type != right->columns[0].type) fail(GX_EINVAL, "Join columns cannot have different types");
     if (left->num_columns == 1 || right->num_columns == 1)
         fail(GX_EINVAL, "Left and right table should have at least 1 payload column");
-    // HASH and PARTITION (hash_join.cu, partition_hash_join.cu in the
-    // reference) return the same pairs as SORT; here all three run the one
-    // matcher above (dense placement or sorted build + radix directory),
-    // which is this library's fastest plan for every key shape it handles.
     if (hint->join_algo != GX_JOIN_SORT && hint->join_algo != GX_JOIN_HASH && hint->join_algo != GX_JOIN_PARTITION)
         fail(GX_EINVAL, "Unsupported join algorithm");
     join_inputs in;
@@ -721,7 +690,7 @@ void inner_eq_join(const gx_table_view* left, const gx_table_view* right, const 
         in.rpay.push_back(resolve(right->columns[c]));
         require(in.rpay.back().n == in.rkey.n, "join: right payload length differs from key length");
     }
-    join_core(in, *hint, false, s, out);
+    run_join(in, *hint, false, s, out);
 }
 
 void inner_eq_join_rowids(const gx_column_view& l, const gx_column_view& r, const gx_join_hint* hint,
@@ -733,7 +702,7 @@ void inner_eq_join_rowids(const gx_column_view& l, const gx_column_view& r, cons
     if (hint) h = *hint;
     else { std::memset(&h, 0, sizeof(h)); h.join_algo = GX_JOIN_SORT; h.mat_algo = GX_MAT_GFUR; }
     if (h.max_out > GX_MAX_JOIN_OUTPUT_SIZE) fail(GX_EINVAL, "Output size exceeds the maximum limit");
-    join_core(in, h, true, s, out);
+    run_join(in, h, true, s, out);
 }
 
 }  // namespace gx

@@ -17,7 +17,7 @@ import pytest
 
 import eiger_b200 as gx
 import oracle as O
-from tests.helpers import FLOAT_RTOL, assert_columns_match, sort_by_key
+from tests.helpers import assert_columns_match, sort_by_key
 
 pytestmark = pytest.mark.gpu
 
@@ -108,11 +108,6 @@ def test_groupby_2p28_rows_hard_corners(kdt, groups, zipf_s):
         c.free()
 
 
-def float_sum_error_bound_is_met(got, exp):
-    rel = np.abs(got - exp) / np.maximum(np.abs(exp), 1e-300)
-    return float(rel.max()) <= FLOAT_RTOL
-
-
 # ---------------------------------------------------------------- join ----
 def check_unique_build_join(bk, pk, hint):
     """Full pair-set check of a join whose build side (left) has unique keys."""
@@ -146,6 +141,20 @@ def test_join_2p28_probe_zipf_1():
     del zr, cdf
     m = check_unique_build_join(bk, pk, gx.make_join_hint(gx.JOIN_SORT, gx.MAT_GFUR, unique_left=1))
     assert m == npr
+
+
+@pytest.mark.parametrize("algo", [gx.JOIN_HASH, gx.JOIN_PARTITION])
+def test_join_2p28_probe_hash_plans(algo):
+    # The benchmark's join (2^24 unique build keys, 2^28 probe keys, 10%
+    # absent) through the hash multiset and the partitioned hash join.
+    import torch
+    nb, npr = 1 << 24, 1 << 28
+    bk = torch.empty(nb, dtype=torch.int32, device="cuda")
+    gx.generate_permutation(bk, 42)
+    pk = torch.empty(npr, dtype=torch.int32, device="cuda")
+    gx.generate_keys(pk, gx.gen_spec(seed=39, groups=nb, miss_frac=0.1))
+    m = check_unique_build_join(bk, pk, gx.make_join_hint(algo, gx.MAT_GFUR, unique_left=1))
+    assert abs(m - 0.9 * npr) < 0.01 * npr
 
 
 @pytest.mark.parametrize("mode", [gx.SORTED_BUILD, gx.SORT_MERGE])
