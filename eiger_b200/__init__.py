@@ -33,6 +33,8 @@ MAT_AUTO, MAT_GFUR, MAT_GFTR, MAT_INDEX_CLUSTER = range(4)
 SORTED_BUILD, SORT_MERGE = 0, 1
 ASCENDING, DESCENDING = 0, 1
 SELECT_HEURISTIC, SELECT_LEARNED = 0, 1
+CMP_LT, CMP_LE, CMP_GT, CMP_GE, CMP_EQ, CMP_NE, CMP_BETWEEN = range(7)
+COMBINE_AND, COMBINE_OR = 0, 1
 DIST_UNIFORM, DIST_CYCLIC, DIST_ZIPF, DIST_SEQUENCE, DIST_ZIPF_APPROX = range(5)
 
 STATUS = {0: "GX_OK", 1: "GX_EINVAL", 2: "GX_ENOMEM", 3: "GX_ECUDA", 4: "GX_EOVERFLOW",
@@ -96,6 +98,11 @@ class GenSpec(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("stream_id", C.c_uint64), ("dist", C.c_int32), ("scatter", C.c_int32),
                 ("groups", C.c_int64), ("zipf_s", C.c_double), ("zipf_cdf", C.c_void_p), ("lo", C.c_int64),
                 ("hi", C.c_int64), ("miss_frac", C.c_double)]
+
+
+class Predicate(C.Structure):
+    _fields_ = [("column_index", C.c_int64), ("op", C.c_int32), ("reserved", C.c_int32), ("lo_i", C.c_int64),
+                ("hi_i", C.c_int64), ("lo_f", C.c_double), ("hi_f", C.c_double)]
 
 
 class BatchInstance(C.Structure):
@@ -174,6 +181,12 @@ def _load() -> C.CDLL:
         "gx_batch_results": ([vp, C.POINTER(BatchResult)], i32),
         "gx_batch_tuning": ([vp, C.POINTER(i32), C.POINTER(i32)], i32),
         "gx_batch_plan_free": ([vp], None),
+        "gx_multikey_compress": ([tv, i32, vp, oc, C.POINTER(i32)], i32),
+        "gx_gather": ([cv, cv, vp, oc], i32),
+        "gx_select_to_bitmask": ([tv, C.POINTER(Predicate), i32, i32, vp, oc], i32),
+        "gx_select": ([tv, C.POINTER(Predicate), i32, i32, vp, C.POINTER(vp)], i32),
+        "gx_compact": ([tv, cv, vp, C.POINTER(vp)], i32),
+        "gx_count_nonzero": ([cv, vp, C.POINTER(i64)], i32),
     }
     for name in ("gx_groupby", "gx_groupby_hash", "gx_groupby_sort", "gx_groupby_sort_gfur",
                  "gx_groupby_partition", "gx_groupby_partition_gfur"):
@@ -238,11 +251,64 @@ def view(t, gx_type: int | None = None, offset: int = 0) -> ColumnView:
     return ColumnView(t.data_ptr(), n - offset, ty, offset)
 
 
+class StringColumn:
+    """A device STRING column in the ARROW layout: `chars` (uint8 tensor) and
+    `offsets` (int64 tensor, rows + 1 entries); `row_offset` skips rows like
+    a column view's offset.  Usable wherever a key column is accepted."""
+
+    def __init__(self, chars, offsets, rows: int | None = None, row_offset: int = 0):
+        self.chars, self.offsets = chars, offsets
+        self.row_offset = row_offset
+        self.rows = (offsets.numel() - 1 - row_offset) if rows is None else rows
+        self._sc = StringColumns(chars.data_ptr(), offsets.data_ptr())
+
+    def view(self) -> ColumnView:
+        return ColumnView(C.cast(C.pointer(self._sc), C.c_void_p), self.rows, STRING, self.row_offset)
+
+    @staticmethod
+    def from_list(strs: Sequence[bytes]) -> "StringColumn":
+        """Uploads a list of byte strings."""
+        torch = _torch()
+        lens = np.array([len(x) for x in strs], dtype=np.int64)
+        off = np.zeros(len(strs) + 1, dtype=np.int64)
+        np.cumsum(lens, out=off[1:])
+        chars = np.frombuffer(b"".join(strs), dtype=np.uint8) if off[-1] else np.zeros(1, np.uint8)
+        return StringColumn(torch.from_numpy(chars.copy()).cuda(), torch.from_numpy(off).cuda(), len(strs))
+
+
+def _column_view(c) -> ColumnView:
+    if isinstance(c, ColumnView):
+        return c
+    if isinstance(c, StringColumn):
+        return c.view()
+    return view(c)
+
+
 def table_view(cols: Sequence) -> tuple[TableView, object]:
     arr = (ColumnView * max(len(cols), 1))()
     for i, c in enumerate(cols):
-        arr[i] = c if isinstance(c, ColumnView) else view(c)
-    return TableView(arr, len(cols)), arr
+        arr[i] = _column_view(c)
+    return TableView(arr, len(cols)), (arr, list(cols))
+
+
+def strings_from_device(v: ColumnView) -> np.ndarray:
+    """Copies a STRING column view (host gx_string_columns -> device
+    chars / offsets) to a numpy object array of bytes."""
+    n = v.size
+    if n == 0:
+        return np.array([], dtype=object)
+    sc = C.cast(v.data, C.POINTER(StringColumns)).contents
+    off = np.empty(n + 1, dtype=np.int64)
+    check(lib.gx_copy(off.ctypes.data, sc.offsets + 8 * v.offset, off.nbytes, None))
+    chars = np.empty(max(int(off[-1] - off[0]), 1), dtype=np.uint8)
+    if off[-1] > off[0]:
+        check(lib.gx_copy(chars.ctypes.data, sc.chars + int(off[0]), int(off[-1] - off[0]), None))
+    b = chars.tobytes()
+    base = int(off[0])
+    out = np.empty(n, dtype=object)
+    for i in range(n):
+        out[i] = b[off[i] - base:off[i + 1] - base]
+    return out
 
 
 def _stream_ptr(stream) -> int | None:
@@ -283,6 +349,8 @@ class Table:
 
     def to_numpy(self, i: int) -> np.ndarray:
         v = self.column(i)
+        if v.type == STRING:
+            return strings_from_device(v)
         out = np.empty(v.size, dtype=_NP[v.type])
         if v.size:
             check(lib.gx_copy(out.ctypes.data, v.data, out.nbytes, None))
@@ -339,6 +407,74 @@ def groupby(keys: Sequence, vals: Sequence, requests: Iterable[tuple[int, int]],
     fn = getattr(lib, _GROUPBY_FN[entry])
     check(fn(C.byref(ktv), C.byref(vtv), arr, len(reqs), C.byref(hint), _stream_ptr(stream), C.byref(out)))
     return Table(out.value)
+
+
+def distinct(keys: Sequence, hint: GroupbyHint | None = None, algo: int = HASH, stream=None) -> Table:
+    """hash::distinct / sort::distinct: one row per distinct key row."""
+    hint = hint if hint is not None else make_hint(algo)
+    ktv, _k = table_view(keys)
+    out = C.c_void_p()
+    fn = lib.gx_distinct_sort if algo in (SORT, SORT_OPT, SORT_GFUR) else lib.gx_distinct_hash
+    check(fn(C.byref(ktv), C.byref(hint), _stream_ptr(stream), C.byref(out)))
+    return Table(out.value)
+
+
+def aggregate(cols: Sequence, requests: Iterable[tuple[int, int]], stream=None) -> Table:
+    """groupby::aggregate::aggregate: one-row table of whole-column aggregates."""
+    tv, _t = table_view(cols)
+    reqs = list(requests)
+    arr = (AggRequest * max(len(reqs), 1))(*[AggRequest(c, k) for c, k in reqs])
+    out = C.c_void_p()
+    check(lib.gx_aggregate(C.byref(tv), arr, len(reqs), _stream_ptr(stream), C.byref(out)))
+    return Table(out.value)
+
+
+def predicate(column: int, op: int, lo=0, hi=0) -> Predicate:
+    """column (op) literal; BETWEEN keeps lo <= x < hi.  The literal is used
+    as an integer for integer columns and as a double for float columns."""
+    def i64(x):  # uint64 literals above 2^63 travel as their two's-complement bits
+        x = int(x)
+        return x - (1 << 64) if x >= (1 << 63) else x
+
+    p = Predicate()
+    p.column_index, p.op = column, op
+    p.lo_f, p.hi_f = float(lo), float(hi)
+    p.lo_i, p.hi_i = i64(lo), i64(hi)
+    return p
+
+
+def _preds(preds):
+    return (Predicate * max(len(preds), 1))(*preds), len(preds)
+
+
+def select_to_bitmask(cols: Sequence, preds: Sequence[Predicate], combine=COMBINE_AND, stream=None):
+    tv, _t = table_view(cols)
+    arr, n = _preds(preds)
+    o = OwnedColumn()
+    check(lib.gx_select_to_bitmask(C.byref(tv), arr, n, combine, _stream_ptr(stream), C.byref(o)))
+    return owned_to_torch(o)
+
+
+def select(cols: Sequence, preds: Sequence[Predicate], combine=COMBINE_AND, stream=None) -> Table:
+    tv, _t = table_view(cols)
+    arr, n = _preds(preds)
+    out = C.c_void_p()
+    check(lib.gx_select(C.byref(tv), arr, n, combine, _stream_ptr(stream), C.byref(out)))
+    return Table(out.value)
+
+
+def compact(cols: Sequence, mask, stream=None) -> Table:
+    tv, _t = table_view(cols)
+    out = C.c_void_p()
+    check(lib.gx_compact(C.byref(tv), view(mask, BOOL8 if mask.element_size() == 1 else None),
+                         _stream_ptr(stream), C.byref(out)))
+    return Table(out.value)
+
+
+def count_nonzero(col, stream=None) -> int:
+    c = C.c_int64()
+    check(lib.gx_count_nonzero(view(col), _stream_ptr(stream), C.byref(c)))
+    return int(c.value)
 
 
 def make_join_hint(join_algo=JOIN_SORT, mat_algo=MAT_GFUR, **kw) -> JoinHint:
@@ -439,6 +575,39 @@ def dictionary_encode_strings(chars, offsets, rows: int | None = None, row_offse
     o, nd = OwnedColumn(), C.c_int64()
     check(lib.gx_dictionary_encode_strings(v, size_hint, _stream_ptr(stream), C.byref(o), C.byref(nd)))
     return owned_to_torch(o), nd.value
+
+
+def multikey_compress(keys: Sequence, max_bits: int = 64, stream=None):
+    """Smart key fusion of integral key columns: (UINT64 tensor, bits used),
+    or None when the keys cannot be fused (compress::multikey_compress)."""
+    tv, _keep = table_view(keys)
+    o, bits = OwnedColumn(), C.c_int32()
+    st = lib.gx_multikey_compress(C.byref(tv), max_bits, _stream_ptr(stream), C.byref(o), C.byref(bits))
+    if st == 6:  # GX_EUNSUPPORTED: not compressible
+        return None
+    check(st)
+    return owned_to_torch(o), bits.value
+
+
+def gather(gather_map, col, stream=None):
+    """out[i] = col[gather_map[i]] (util::device::gather); STRING columns
+    (StringColumn) come back as a numpy object array of bytes."""
+    o = OwnedColumn()
+    check(lib.gx_gather(view(gather_map), _column_view(col), _stream_ptr(stream), C.byref(o)))
+    if o.type != STRING:
+        return owned_to_torch(o)
+    n = o.size
+    off = np.empty(n + 1, dtype=np.int64)
+    check(lib.gx_copy(off.ctypes.data, o.data, off.nbytes, None))
+    chars = np.empty(max(int(off[-1]), 1), dtype=np.uint8)
+    if off[-1]:
+        check(lib.gx_copy(chars.ctypes.data, o.data + 8 * (n + 1), int(off[-1]), None))
+    check(lib.gx_free(o.data, None))
+    b = chars.tobytes()
+    out = np.empty(n, dtype=object)
+    for i in range(n):
+        out[i] = b[off[i]:off[i + 1]]
+    return out
 
 
 def compute_ndv_approx(col, stream=None) -> int:

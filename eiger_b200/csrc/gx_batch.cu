@@ -545,8 +545,8 @@ static void batch_run_plain(gx_batch_plan* p, cudaStream_t s) {
 // dictionary_encode rejects STRING, dictionary_encode.cu:32-34).  The table
 // is the plain engine's (hash tag + representative row per slot); without a
 // size hint it starts at 2^22 distinct strings and grows by 4x on overflow.
-static void dictionary_encode_strings(const gx_column_view& v, int64_t size_hint, cudaStream_t s, gx_column* out,
-                                      int64_t* ndv) {
+void dictionary_encode_strings(const gx_column_view& v, int64_t size_hint, cudaStream_t s, gx_column* out,
+                               int64_t* ndv) {
     require(v.type == GX_STRING, "dictionary_encode_strings: STRING column required");
     require(v.size >= 0 && v.offset >= 0, "dictionary_encode_strings: negative size or offset");
     const int64_t rows = v.size;

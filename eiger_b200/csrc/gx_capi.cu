@@ -101,7 +101,8 @@ gx_status gx_table_column(const gx_table* t, int64_t i, gx_column_view* out) {
         gx::require(t && out, "null argument");
         gx::require(i >= 0 && i < (int64_t)t->cols.size(), "column out of range");
         gx::require(t->cols[i].present, "column was released");
-        out->data = t->cols[i].buf.get();
+        // A STRING column's view points to its host-side (chars, offsets) pair.
+        out->data = t->cols[i].type == GX_STRING ? (void*)t->cols[i].str.get() : t->cols[i].buf.get();
         out->size = t->cols[i].size;
         out->type = t->cols[i].type;
         out->offset = 0;
@@ -207,6 +208,66 @@ gx_status gx_aggregate(const gx_table_view* input, const gx_agg_request* req, in
         std::unique_ptr<gx_table> t(new gx_table);
         gx::aggregate_dispatch(input, req, n, cs(s), t.get());
         *out = t.release();
+    })
+}
+
+gx_status gx_select_to_bitmask(const gx_table_view* table, const gx_predicate* preds, int32_t n, int32_t combine,
+                               gx_stream_t s, gx_column* mask) {
+    GX_TRY({
+        gx::require(mask != nullptr, "null output");
+        gx::select_to_bitmask(table, preds, n, combine, cs(s), mask);
+    })
+}
+
+gx_status gx_select(const gx_table_view* table, const gx_predicate* preds, int32_t n, int32_t combine, gx_stream_t s,
+                    gx_table** out) {
+    GX_TRY({
+        gx::require(out != nullptr, "null output");
+        std::unique_ptr<gx_table> t(new gx_table);
+        gx::select_rows(table, preds, n, combine, cs(s), t.get());
+        *out = t.release();
+    })
+}
+
+gx_status gx_compact(const gx_table_view* input, gx_column_view mask, gx_stream_t s, gx_table** out) {
+    GX_TRY({
+        gx::require(out != nullptr, "null output");
+        std::unique_ptr<gx_table> t(new gx_table);
+        gx::compact_by_mask(input, mask, cs(s), t.get());
+        *out = t.release();
+    })
+}
+
+gx_status gx_count_nonzero(gx_column_view column, gx_stream_t s, int64_t* count) {
+    GX_TRY({
+        gx::require(count != nullptr, "null output");
+        *count = gx::count_nonzero(column, cs(s));
+    })
+}
+
+gx_status gx_multikey_compress(const gx_table_view* key, int32_t max_bits, gx_stream_t s, gx_column* out,
+                               int32_t* total_bits) {
+    GX_TRY({
+        gx::require(key && out, "null argument");
+        gx::require(max_bits >= 1 && max_bits <= 64, "multikey_compress: max_fused_key_bits must be in 1..64");
+        gx::owned_col fused;
+        int bits = 0;
+        if (!gx::multikey_compress(key, max_bits, cs(s), &fused, &bits))
+            gx::fail(GX_EUNSUPPORTED, "multikey_compress: keys are not all integral or need more than " +
+                                          std::to_string(max_bits) + " bits");
+        if (total_bits) *total_bits = bits;
+        *out = gx::to_gx_column(std::move(fused));
+    })
+}
+
+gx_status gx_gather(gx_column_view gather_map, gx_column_view input, gx_stream_t s, gx_column* out) {
+    GX_TRY({
+        gx::require(out != nullptr, "null output");
+        gx::require(gather_map.type == GX_INT64, "gather: the gather map must be INT64 row ids");
+        col m = resolve(gather_map);
+        gx::owned_col o = gx::gather_column(input, m.as<int64_t>(), m.n, cs(s));
+        GX_CUDA(cudaStreamSynchronize(cs(s)));
+        *out = gx::to_gx_column(std::move(o));
     })
 }
 

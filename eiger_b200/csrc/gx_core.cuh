@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <memory>
@@ -138,6 +139,15 @@ public:
         bytes_ = 0;
     }
     void* release() { void* p = p_; p_ = nullptr; bytes_ = 0; return p; }
+    // Takes ownership of a buffer this pool handed out earlier (e.g. through
+    // a released gx_column).
+    static dbuf adopt(void* p, size_t bytes, cudaStream_t s) {
+        dbuf d;
+        d.p_ = p;
+        d.s_ = s;
+        d.bytes_ = bytes;
+        return d;
+    }
     template <typename T = void>
     T* get() const { return static_cast<T*>(p_); }
     size_t bytes() const { return bytes_; }
@@ -194,11 +204,15 @@ inline col resolve(const gx_column_view& v) {
 // ---------------------------------------------------------------------------
 // Owned columns / tables returned through the C ABI.
 // ---------------------------------------------------------------------------
+// A STRING column owns one buffer: the rows + 1 int64 offsets followed by
+// the characters (ARROW layout); `str` is the host-side pair of device
+// pointers that views of the column point to.
 struct owned_col {
     dbuf buf;
     int64_t size = 0;
     int type = GX_EMPTY;
     bool present = true;
+    std::unique_ptr<gx_string_columns> str;
 };
 
 }  // namespace gx
@@ -216,6 +230,16 @@ inline owned_col make_col(int type, int64_t rows, cudaStream_t s, int64_t capaci
     int64_t cap = capacity_rows < 0 ? rows : capacity_rows;
     size_t bytes = (size_t)cap * size_of(type);
     if (bytes) c.buf = dbuf(bytes, s);
+    return c;
+}
+// STRING column of `rows` strings holding `char_bytes` characters in total.
+inline owned_col make_string_col(int64_t rows, int64_t char_bytes, cudaStream_t s) {
+    owned_col c;
+    c.type = GX_STRING;
+    c.size = rows;
+    const size_t off_bytes = (size_t)(rows + 1) * 8;
+    c.buf = dbuf(off_bytes + (size_t)std::max<int64_t>(char_bytes, 1), s);
+    c.str.reset(new gx_string_columns{c.buf.get<char>() + off_bytes, c.buf.get<int64_t>()});
     return c;
 }
 inline gx_column to_gx_column(owned_col&& c) {

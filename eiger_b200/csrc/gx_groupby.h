@@ -70,5 +70,38 @@ void key_image_range(const col& keys, uint64_t* lo, uint64_t* hi, cudaStream_t s
 
 // ----- statistics (gx_hll.cu) -----
 int64_t ndv_estimate(const col& key, cudaStream_t s);
+// Min / max of a numeric column, widened to int64 (integers) or double
+// bits (floats) (gx_hll.cu).
+void compute_min_max(const col& key, void* min_out, void* max_out, cudaStream_t s);
+
+// ----- dictionary encoding (gx_dict.cu, gx_batch.cu) -----
+// mode 0: hash codes (first-insert order), 1: order-preserving codes.
+void dictionary_encode(const gx_column_view& v, int encode_type, int64_t size_hint, double load_factor, int mode,
+                       cudaStream_t s, gx_column* out, int64_t* dict_size);
+// ARROW string column -> int32 codes dense in [0, NDV).
+void dictionary_encode_strings(const gx_column_view& v, int64_t size_hint, cudaStream_t s, gx_column* out,
+                               int64_t* ndv);
+
+// ----- keys that are not one numeric column (gx_keys.cu) -----
+// One int64 / uint64 key per row that is equal exactly when all key
+// columns are equal.  With `skf`, integral columns are bit-packed by value
+// range (the reference's smart key fusion); otherwise, or when packing
+// does not fit 64 bits, columns are dictionary-encoded and chained.
+// *groups_bound gets an upper bound of the distinct keys.
+owned_col derive_group_key(const gx_table_view* key, bool skf, cudaStream_t s, int64_t* groups_bound);
+// Bit-packs integral key columns by value range into one UINT64 column
+// (src/cuda/compress/multikey_compress.cu:25-399); returns false when a
+// column is not integral or the packed key needs more than max_bits.
+bool multikey_compress(const gx_table_view* key, int max_bits, cudaStream_t s, owned_col* out, int* total_bits);
+// ----- filter (gx_select.cu) -----
+void select_to_bitmask(const gx_table_view* t, const gx_predicate* preds, int n, int combine, cudaStream_t s,
+                       gx_column* mask);
+void select_rows(const gx_table_view* t, const gx_predicate* preds, int n, int combine, cudaStream_t s,
+                 gx_table* out);
+void compact_by_mask(const gx_table_view* t, const gx_column_view& mask, cudaStream_t s, gx_table* out);
+int64_t count_nonzero(const gx_column_view& v, cudaStream_t s);
+
+// out = column v gathered at row ids idx[0..n) (numeric or STRING).
+owned_col gather_column(const gx_column_view& v, const int64_t* idx, int64_t n, cudaStream_t s);
 
 }  // namespace gx

@@ -12,7 +12,11 @@
 //   operators/join/join.hpp, inner_join.hpp               join_hint, inner_eq_join()
 //   operators/sort/sort.hpp:14-75       sort_column_pair, sort_column, argsort
 //   operators/partition/partition.hpp   partition_column_pair, ..., compute_partition_offsets
-//   compress/dictionary_encode.hpp      dictionary_encode{,_with_order}, ready-dictionary overload
+//   compress/dictionary_encode.hpp      dictionary_encode{,_with_order}, ready-dictionary and table overloads
+//   compress/multikey_compress.hpp      multikey_compress (smart key fusion)
+//   operators/groupby/aggregation.hpp   aggregate::aggregate; groupby_{hash,sort}.hpp distinct
+//   utils/transform.hpp                 util::device::gather, compact, count_nonzero
+//   operators/select/select.hpp         select / select_to_bitmask over predicate lists
 // Error convention: a non-OK status throws std::bad_alloc for GX_ENOMEM and
 // std::runtime_error otherwise (the reference's exception types).  Results
 // are owned device columns freed through gx_free.
@@ -112,8 +116,16 @@ public:
 // Owning device column (buffer from the library's stream-ordered pool).
 class column {
 public:
+    // A STRING column's buffer holds its size+1 int64 offsets followed by the
+    // characters (ARROW layout); its views point to a host-side
+    // gx_string_columns pair, as the reference's string views point to a
+    // (chars, offsets) helper (string/string_column.hpp:22-90).
     column(data_type type, size_type size, void* data, size_type capacity_bytes)
-        : _type(type), _size(size), _data(data), _bytes(capacity_bytes) {}
+        : _type(type), _size(size), _data(data), _bytes(capacity_bytes) {
+        if (type.id() == type_id::STRING)
+            _str.reset(new gx_string_columns{static_cast<const char*>(data) + (size + 1) * 8,
+                                             static_cast<const int64_t*>(data)});
+    }
     explicit column(gx_column c) : column(data_type{(type_id)c.type}, c.size, c.data, c.capacity_bytes) {}
     column(data_type type, size_type num_rows, bool clear = false, cudaStream_t stream = 0)
         : _type(type), _size(num_rows) {
@@ -123,7 +135,8 @@ public:
     }
     column(const column&) = delete;
     column& operator=(const column&) = delete;
-    column(column&& o) noexcept : _type(o._type), _size(o._size), _data(o._data), _bytes(o._bytes) {
+    column(column&& o) noexcept
+        : _type(o._type), _size(o._size), _data(o._data), _bytes(o._bytes), _str(std::move(o._str)) {
         o._data = nullptr;
         o._size = 0;
     }
@@ -136,14 +149,19 @@ public:
     size_type bytes() const noexcept { return _bytes; }
     template <typename T = void>
     T* data() const noexcept { return static_cast<T*>(_data); }
-    column_view view(size_type offset = 0) const { return column_view(_data, _size, _type, offset); }
-    mutable_column_view mutable_view(size_type offset = 0) { return mutable_column_view(_data, _size, _type, offset); }
+    column_view view(size_type offset = 0) const {
+        return column_view(_str ? static_cast<void*>(_str.get()) : _data, _size, _type, offset);
+    }
+    mutable_column_view mutable_view(size_type offset = 0) {
+        return mutable_column_view(_str ? static_cast<void*>(_str.get()) : _data, _size, _type, offset);
+    }
 
 private:
     data_type _type;
     size_type _size{0};
     void* _data{nullptr};
     size_type _bytes{0};
+    std::unique_ptr<gx_string_columns> _str;
 };
 using column_ptr = std::unique_ptr<column>;
 
@@ -165,6 +183,11 @@ public:
     void add_column(column_view_t c) {
         if (c.size() != num_rows()) throw std::runtime_error("New column must have the same number of rows as the table");
         _columns.push_back(c);
+    }
+    table_view_base select_columns(std::vector<size_type> const& idx) const {
+        std::vector<column_view_t> cols;
+        for (auto i : idx) cols.push_back(_columns.at(i));
+        return table_view_base(cols);
     }
     std::vector<gx_column_view> to_gx() const {
         std::vector<gx_column_view> v;
@@ -279,10 +302,31 @@ inline std::unique_ptr<table> groupby(table_view key, table_view val, std::vecto
                                       groupby_hint& hint, cudaStream_t stream = 0) {
     return detail::run(gx_groupby, key, val, reqs, hint, stream);
 }
+namespace detail {
+using distinct_fn_t = gx_status (*)(const gx_table_view*, gx_groupby_hint*, gx_stream_t, gx_table**);
+inline std::unique_ptr<table> run_distinct(distinct_fn_t fn, table_view key, groupby_hint& hint, cudaStream_t stream) {
+    gamax::detail::gx_tv k(key);
+    gx_groupby_hint h;
+    gx_groupby_hint_init(&h);
+    h.groups_upper_bound = hint.groups_upper_bound;
+    h.groupby_algo = (int32_t)hint.groupby_algo;
+    h.enable_skf = hint.enable_skf;
+    gx_table* out = nullptr;
+    gamax::detail::check(fn(&k.tv, &h, gamax::detail::gs(stream), &out));
+    hint.groupby_algo = (groupby_algo)h.groupby_algo;
+    return gamax::detail::adopt(out);
+}
+}  // namespace detail
+
 namespace hash {
 inline std::unique_ptr<table> groupby(table_view key, table_view val, std::vector<aggregation_request>& reqs,
                                       groupby_hint& hint, cudaStream_t stream = 0) {
     return detail::run(gx_groupby_hash, key, val, reqs, hint, stream);
+}
+// One row per distinct key row (groupby_hash.hpp:24-34); STRING and
+// multi-column keys included.
+inline std::unique_ptr<table> distinct(table_view key, groupby_hint& hint, cudaStream_t stream = 0) {
+    return detail::run_distinct(gx_distinct_hash, key, hint, stream);
 }
 }  // namespace hash
 namespace sort {
@@ -293,6 +337,10 @@ inline std::unique_ptr<table> groupby(table_view key, table_view val, std::vecto
 inline std::unique_ptr<table> groupby_gfur(table_view key, table_view val, std::vector<aggregation_request>& reqs,
                                            groupby_hint& hint, cudaStream_t stream = 0) {
     return detail::run(gx_groupby_sort_gfur, key, val, reqs, hint, stream);
+}
+// Sort-based distinct (groupby_sort.hpp:31-47).
+inline std::unique_ptr<table> distinct(table_view key, groupby_hint& hint, cudaStream_t stream = 0) {
+    return detail::run_distinct(gx_distinct_sort, key, hint, stream);
 }
 }  // namespace sort
 namespace partition {
@@ -305,6 +353,19 @@ inline std::unique_ptr<table> groupby_gfur(table_view key, table_view val, std::
     return detail::run(gx_groupby_partition_gfur, key, val, reqs, hint, stream);
 }
 }  // namespace partition
+
+// Whole-table aggregates, one output row (aggregation.hpp:32-37).
+namespace aggregate {
+inline std::unique_ptr<table> aggregate(table_view input, std::vector<aggregation_request>& reqs,
+                                        cudaStream_t stream = 0) {
+    gamax::detail::gx_tv t(input);
+    std::vector<gx_agg_request> r;
+    for (auto& q : reqs) r.push_back(gx_agg_request{q.column_index, (int32_t)q.agg_kind});
+    gx_table* out = nullptr;
+    gamax::detail::check(gx_aggregate(&t.tv, r.data(), (int32_t)r.size(), gamax::detail::gs(stream), &out));
+    return gamax::detail::adopt(out);
+}
+}  // namespace aggregate
 }  // namespace groupby
 
 // --------------------------------------------------------------------- join
@@ -366,6 +427,22 @@ inline std::pair<std::unique_ptr<column>, std::unique_ptr<column>> argsort(
                                     gamax::detail::gs(stream), &k, &i));
     return {std::make_unique<column>(k), std::make_unique<column>(i)};
 }
+// gamax::column& overloads (sort.hpp:14-75): the same sorts on the column's view.
+inline std::pair<std::unique_ptr<column>, std::unique_ptr<column>> sort_column_pair(
+    column& key, column& val, int begin_bit = 0, int end_bit = -1, sort_order order = sort_order::ASCENDING,
+    void* d_temp = nullptr, size_t temp_bytes = 0, cudaStream_t stream = 0) {
+    return sort_column_pair(key.view(), val.view(), begin_bit, end_bit, order, d_temp, temp_bytes, stream);
+}
+inline std::unique_ptr<column> sort_column(column& col, int begin_bit = 0, int end_bit = -1,
+                                           sort_order order = sort_order::ASCENDING, void* d_temp = nullptr,
+                                           size_t temp_bytes = 0, cudaStream_t stream = 0) {
+    return sort_column(col.view(), begin_bit, end_bit, order, d_temp, temp_bytes, stream);
+}
+inline std::pair<std::unique_ptr<column>, std::unique_ptr<column>> argsort(
+    column& col, int begin_bit = 0, int end_bit = -1, sort_order order = sort_order::ASCENDING,
+    void* d_temp = nullptr, size_t temp_bytes = 0, cudaStream_t stream = 0) {
+    return argsort(col.view(), begin_bit, end_bit, order, d_temp, temp_bytes, stream);
+}
 }  // namespace sort
 
 // ---------------------------------------------------------------- partition
@@ -399,6 +476,24 @@ inline std::unique_ptr<column> compute_partition_offsets(column_view col, int be
     gamax::detail::check(gx_compute_partition_offsets(col.to_gx(), begin_bit, end_bit, gamax::detail::gs(stream), &o));
     return std::make_unique<column>(o);
 }
+// gamax::column& overloads (partition.hpp:11-45).
+inline std::pair<std::unique_ptr<column>, std::unique_ptr<column>> partition_column_pair(
+    column& key, column& val, int begin_bit, int end_bit, void* d_temp = nullptr, size_t temp_bytes = 0,
+    cudaStream_t stream = 0) {
+    return partition_column_pair(key.view(), val.view(), begin_bit, end_bit, d_temp, temp_bytes, stream);
+}
+inline std::unique_ptr<column> partition_column(column& col, int begin_bit, int end_bit, void* d_temp = nullptr,
+                                                size_t temp_bytes = 0, cudaStream_t stream = 0) {
+    return partition_column(col.view(), begin_bit, end_bit, d_temp, temp_bytes, stream);
+}
+inline std::pair<std::unique_ptr<column>, std::unique_ptr<column>> arg_partition(
+    column& col, int begin_bit, int end_bit, void* d_temp = nullptr, size_t temp_bytes = 0, cudaStream_t stream = 0) {
+    return arg_partition(col.view(), begin_bit, end_bit, d_temp, temp_bytes, stream);
+}
+inline std::unique_ptr<column> compute_partition_offsets(column& col, int begin_bit, int end_bit,
+                                                         cudaStream_t stream = 0) {
+    return compute_partition_offsets(col.view(), begin_bit, end_bit, stream);
+}
 }  // namespace partition
 
 // ----------------------------------------------------------------- compress
@@ -429,7 +524,105 @@ inline std::unique_ptr<column> dictionary_encode(const column_view col, const co
                                                         gamax::detail::gs(stream), &c));
     return std::make_unique<column>(c);
 }
+// The table overload rejects every table, as the reference's does
+// (dictionary_encode.cu:41-43, 376-384).
+inline std::pair<std::unique_ptr<column>, size_type> dictionary_encode(
+    const table_view, const data_type = data_type{type_id::INT32}, const size_type = 0, const double = 0.25,
+    cudaStream_t = 0) {
+    throw std::runtime_error("Cannot dictionary encode table");
+}
+
+struct multikey_compress_options {
+    bool always_compress = true;
+    int max_fused_key_bits = 64;
+    int* out_total_bits = nullptr;
+};
+// Smart key fusion (multikey_compress.hpp:29-32): nullptr when the keys
+// cannot be packed into max_fused_key_bits bits.
+inline std::unique_ptr<column> multikey_compress(table_view table, multikey_compress_options const& options = {},
+                                                 cudaStream_t stream = 0) {
+    gamax::detail::gx_tv t(table);
+    gx_column c;
+    int32_t bits = 0;
+    gx_status st = gx_multikey_compress(&t.tv, options.max_fused_key_bits, gamax::detail::gs(stream), &c, &bits);
+    if (st == GX_EUNSUPPORTED) return nullptr;
+    gamax::detail::check(st);
+    if (options.out_total_bits) *options.out_total_bits = bits;
+    return std::make_unique<column>(c);
+}
 }  // namespace compress
+
+// ----------------------------------------------------------------- util
+namespace util::device {
+// out[i] = input[gather_map[i]] (utils/transform.hpp, transform.cu:168-186).
+inline std::unique_ptr<column> gather(column_view gather_map, column_view input, cudaStream_t stream = 0) {
+    gx_column c;
+    gamax::detail::check(gx_gather(gather_map.to_gx(), input.to_gx(), gamax::detail::gs(stream), &c));
+    return std::make_unique<column>(c);
+}
+// Rows of every column whose BOOL8 mask byte is nonzero, in order
+// (transform.hpp:34-48).
+inline std::unique_ptr<table> compact(table_view input, column_view mask, cudaStream_t stream = 0) {
+    gamax::detail::gx_tv t(input);
+    gx_table* out = nullptr;
+    gamax::detail::check(gx_compact(&t.tv, mask.to_gx(), gamax::detail::gs(stream), &out));
+    return gamax::detail::adopt(out);
+}
+inline std::unique_ptr<column> compact(column_view input, column_view mask, cudaStream_t stream = 0) {
+    auto t = compact(table_view(std::vector<column_view>{input}), mask, stream);
+    return t->release_column(0);
+}
+inline size_type count_nonzero(column_view input, cudaStream_t stream = 0) {
+    int64_t c = 0;
+    gamax::detail::check(gx_count_nonzero(input.to_gx(), gamax::detail::gs(stream), &c));
+    return c;
+}
+}  // namespace util::device
+
+// ------------------------------------------------------------------ select
+// Filters whose predicate is a list of column-vs-literal comparisons joined
+// by AND or OR (gx_predicate); the reference's select takes general
+// expression trees (select.hpp:15-64), which this library does not build.
+namespace select {
+enum class cmp { LT, LE, GT, GE, EQ, NE, BETWEEN };
+struct predicate {
+    size_type column;
+    cmp op;
+    int64_t lo_i{0}, hi_i{0};
+    double lo_f{0}, hi_f{0};
+    static predicate on_int(size_type c, cmp op, int64_t lo, int64_t hi = 0) {
+        return predicate{c, op, lo, hi, (double)lo, (double)hi};
+    }
+    static predicate on_float(size_type c, cmp op, double lo, double hi = 0) {
+        return predicate{c, op, (int64_t)lo, (int64_t)hi, lo, hi};
+    }
+};
+enum class combine { AND, OR };
+namespace detail {
+inline std::vector<gx_predicate> to_gx(std::vector<predicate> const& ps) {
+    std::vector<gx_predicate> out;
+    for (auto& p : ps) out.push_back(gx_predicate{p.column, (int32_t)p.op, 0, p.lo_i, p.hi_i, p.lo_f, p.hi_f});
+    return out;
+}
+}  // namespace detail
+inline column_ptr select_to_bitmask(table_view table, std::vector<predicate> const& preds,
+                                    combine how = combine::AND, cudaStream_t stream = 0) {
+    gamax::detail::gx_tv t(table);
+    auto q = detail::to_gx(preds);
+    gx_column c;
+    gamax::detail::check(gx_select_to_bitmask(&t.tv, q.data(), (int32_t)q.size(), (int32_t)how,
+                                              gamax::detail::gs(stream), &c));
+    return std::make_unique<column>(c);
+}
+inline std::unique_ptr<table> select(table_view table, std::vector<predicate> const& preds,
+                                     combine how = combine::AND, cudaStream_t stream = 0) {
+    gamax::detail::gx_tv t(table);
+    auto q = detail::to_gx(preds);
+    gx_table* out = nullptr;
+    gamax::detail::check(gx_select(&t.tv, q.data(), (int32_t)q.size(), (int32_t)how, gamax::detail::gs(stream), &out));
+    return gamax::detail::adopt(out);
+}
+}  // namespace select
 
 // -------------------------------------------------------------------- stats
 namespace stats {

@@ -86,7 +86,10 @@ typedef struct gx_table_view {
     int64_t num_columns;
 } gx_table_view;
 
-/* An owned device column handed to the caller (free with gx_free). */
+/* An owned device column handed to the caller (free with gx_free).  A
+ * released GX_STRING column's buffer holds its size+1 int64 offsets
+ * followed by the characters (ARROW layout); the view of a STRING column
+ * still inside a gx_table points to a gx_string_columns owned by the table. */
 typedef struct gx_column {
     void* data;             /* device; NULL when size == 0 */
     int64_t size;           /* rows */
@@ -239,6 +242,70 @@ gx_status gx_aggregate(const gx_table_view* input, const gx_agg_request* request
 
 /* Output type of an aggregation (agg_output_data_type, aggregate.cu:41-53). */
 int32_t gx_agg_output_type(int32_t agg_kind, int32_t input_type);
+
+/* Key tables that are not one numeric column: gx_groupby / gx_distinct_*
+ * accept STRING keys and several key columns (the reference hashes whole
+ * rows, groupby_hash.cu:437-498).  With hint->enable_skf integral key
+ * columns are first packed into one 64-bit key (smart key fusion,
+ * groupby.cu:403-465); the output holds the original key columns, gathered
+ * at one row of each group, then the aggregates. */
+
+/* Smart key fusion: packs integral key columns into one UINT64 column, each
+ * column taking (value - min) on ceil(log2(range + 1)) bits, or its
+ * dictionary code when that is narrower and the range saves fewer than 2/3
+ * of the column's bits; equal packed keys <=> equal key rows.  Returns
+ * GX_EUNSUPPORTED (the reference returns nullptr) when a column is not
+ * integral or the key needs more than max_bits bits; *total_bits gets the
+ * bits used.  Replaces compress::multikey_compress
+ * (compress/multikey_compress.hpp:29-32, multikey_compress.cu:25-399). */
+gx_status gx_multikey_compress(const gx_table_view* key, int32_t max_bits, gx_stream_t stream,
+                               gx_column* out, int32_t* total_bits);
+
+/* out[i] = input[gather_map[i]] for numeric or STRING columns (INT64 row
+ * ids).  Replaces util::device::gather (utils/transform.hpp, transform.cu:168-186)
+ * and the string gather of join materialisation (join/materialize.cu:26-30). */
+gx_status gx_gather(gx_column_view gather_map, gx_column_view input, gx_stream_t stream, gx_column* out);
+
+/* ---------------------------------------------------------------------- */
+/* Filter — gamax::select (src/cuda/operators/select/select.hpp:15-64) and  */
+/* the mask utilities of gamax::util::device (src/cuda/utils/transform.hpp: */
+/* 34-48).  A predicate list compares columns with literals and combines    */
+/* the comparisons with AND or OR (the reference evaluates general          */
+/* expression trees, expr/expr_fast.hpp; those are not part of this ABI).   */
+/* Masks are BOOL8 columns, one byte per row (nonzero = keep).             */
+/* ---------------------------------------------------------------------- */
+typedef enum gx_cmp_op {
+    GX_CMP_LT = 0, GX_CMP_LE = 1, GX_CMP_GT = 2, GX_CMP_GE = 3, GX_CMP_EQ = 4, GX_CMP_NE = 5,
+    GX_CMP_BETWEEN = 6 /* lo <= x < hi */
+} gx_cmp_op;
+typedef enum gx_combine { GX_COMBINE_AND = 0, GX_COMBINE_OR = 1 } gx_combine;
+
+/* column (op) literal.  Integer columns compare with lo_i / hi_i (as
+ * uint64 bits for unsigned columns), float columns with lo_f / hi_f. */
+typedef struct gx_predicate {
+    int64_t column_index;
+    int32_t op;        /* gx_cmp_op */
+    int32_t reserved;
+    int64_t lo_i, hi_i;
+    double lo_f, hi_f;
+} gx_predicate;
+
+/* BOOL8 mask of the rows the predicates keep (select_to_bitmask,
+ * select.hpp:30-34).  1 to 8 predicates on numeric columns. */
+gx_status gx_select_to_bitmask(const gx_table_view* table, const gx_predicate* predicates,
+                               int32_t num_predicates, int32_t combine, gx_stream_t stream,
+                               gx_column* mask);
+/* The kept rows of every column, in input order; the predicates are
+ * evaluated while compacting, so no mask is written (select with
+ * fuse_operations, select.hpp:15-24). */
+gx_status gx_select(const gx_table_view* table, const gx_predicate* predicates,
+                    int32_t num_predicates, int32_t combine, gx_stream_t stream, gx_table** out);
+/* Rows of every (numeric) column whose mask byte is nonzero, in input order
+ * (util::device::compact(table_view, mask), transform.hpp:34-48). */
+gx_status gx_compact(const gx_table_view* input, gx_column_view mask, gx_stream_t stream,
+                     gx_table** out);
+/* Rows whose value is not zero (util::device::count_nonzero). */
+gx_status gx_count_nonzero(gx_column_view column, gx_stream_t stream, int64_t* count);
 
 /* ---------------------------------------------------------------------- */
 /* Inner equi-join — gamax::join (src/cuda/operators/join/join.hpp:7-33,   */

@@ -167,3 +167,16 @@ def test_invalid_arguments_are_rejected_with_messages():
     for call, words in cases:
         assert call() == 1, words
         assert words in gx.last_error()
+
+
+def test_reference_style_caller_compiles_against_all_headers(tmp_path):
+    # The C++ caller of the GPU test (groupby, join, sort / partition on
+    # gamax::column&, dictionary encode, aggregate, phys::*, pullops::*)
+    # compiles and links against the headers and libgx.so without a GPU.
+    from tests.test_cpp_caller_gpu import CALLER
+    src = tmp_path / "caller.cpp"
+    src.write_text(CALLER)
+    cuda = Path("/usr/local/cuda")
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", f"-I{ROOT / 'include'}", f"-I{cuda / 'include'}", str(src),
+                    "-o", str(tmp_path / "caller"), f"-L{ROOT / 'eiger_b200'}", "-lgx", f"-L{cuda / 'lib64'}",
+                    "-lcudart"], check=True)
