@@ -374,19 +374,25 @@ gx_status gx_arg_partition(gx_column_view col_v, int32_t b, int32_t e, void* d_t
 
 namespace gx {
 namespace {
+// Digit histogram of (key >> b) & mask on the raw value (RadixExtractor,
+// src/cuda/operators/partition/partition.cu:103-120): a shared-memory
+// histogram per block for up to 4096 digits, global atomics above that.
 template <typename T>
-__global__ void k_part_offsets(const T* __restrict__ keys, int64_t n, int b, uint64_t mask, int P,
-                               int64_t* __restrict__ out) {
-    // Inclusive offsets of an already partitioned column: out[p] = rows with
-    // digit <= p; digit = (key >> b) & mask on the raw value
-    // (RadixExtractor, src/cuda/operators/partition/partition.cu:103-120).
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t cur = i < n ? (int64_t)(((uint64_t)keys[i] >> b) & mask) : (int64_t)P + 1;
-        int64_t prev = i > 0 ? (int64_t)(((uint64_t)keys[i - 1] >> b) & mask) : -1;
-        // rows < i have digit <= prev; every p in [prev, cur) ends at i
-        for (int64_t p = prev; p < cur; ++p)
-            if (p >= 0) out[p] = i;  // p == P only at i == n: the trailing total
+__global__ void k_digit_hist(const T* __restrict__ keys, int64_t n, int b, uint64_t mask, int P,
+                             unsigned long long* __restrict__ counts) {
+    extern __shared__ unsigned long long sh[];
+    const bool local = P <= 4096;
+    if (local)
+        for (int i = threadIdx.x; i < P; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t d = ((uint64_t)keys[i] >> b) & mask;
+        atomicAdd(local ? &sh[d] : &counts[d], 1ull);
     }
+    __syncthreads();
+    if (local)
+        for (int i = threadIdx.x; i < P; i += blockDim.x)
+            if (sh[i]) atomicAdd(&counts[i], sh[i]);
 }
 }  // namespace
 }  // namespace gx
@@ -399,19 +405,28 @@ extern "C" gx_status gx_compute_partition_offsets(gx_column_view key, int32_t b,
         gx::require(gx::is_signed_int(k.type) || gx::is_unsigned_int(k.type),
                     "Cannot extract radix from non-integral type");
         gx::require(e > b && e - b <= 30, "partition offsets: bad bit range");
+        // Inclusive offsets over the digit histogram, valid for any order of
+        // the keys (HistogramEven + InclusiveSum, partition.cu:122-171):
+        // out[p] = rows with digit <= p, out[P] = rows.
         int P = 1 << (e - b);
         gx::owned_col o = gx::make_col(GX_INT64, P + 1, cs(s));
         uint64_t mask = (uint64_t)P - 1;
-        int g = gx::grid_for(k.n + 1, 256, 8);
-        gx::fill_u64(o.buf.get(), 0, P + 1, cs(s));
-        // Keys are partitioned, so digits are non-decreasing along the column.
-        switch (gx::size_of(k.type)) {
-            case 1: gx::k_part_offsets<<<g, 256, 0, cs(s)>>>(k.as<uint8_t>(), k.n, b, mask, P, o.buf.get<int64_t>()); break;
-            case 2: gx::k_part_offsets<<<g, 256, 0, cs(s)>>>(k.as<uint16_t>(), k.n, b, mask, P, o.buf.get<int64_t>()); break;
-            case 4: gx::k_part_offsets<<<g, 256, 0, cs(s)>>>(k.as<uint32_t>(), k.n, b, mask, P, o.buf.get<int64_t>()); break;
-            default: gx::k_part_offsets<<<g, 256, 0, cs(s)>>>(k.as<uint64_t>(), k.n, b, mask, P, o.buf.get<int64_t>()); break;
+        gx::dbuf counts((size_t)P * 8, cs(s)), ex((size_t)(P + 1) * 8, cs(s));
+        gx::fill_u64(counts.get(), 0, P, cs(s));
+        if (k.n > 0) {
+            const int g = gx::grid_for(k.n, 256, 4);
+            const size_t sh = P <= 4096 ? (size_t)P * 8 : 0;
+            switch (gx::size_of(k.type)) {
+                case 1: gx::k_digit_hist<<<g, 256, sh, cs(s)>>>(k.as<uint8_t>(), k.n, b, mask, P, counts.get<unsigned long long>()); break;
+                case 2: gx::k_digit_hist<<<g, 256, sh, cs(s)>>>(k.as<uint16_t>(), k.n, b, mask, P, counts.get<unsigned long long>()); break;
+                case 4: gx::k_digit_hist<<<g, 256, sh, cs(s)>>>(k.as<uint32_t>(), k.n, b, mask, P, counts.get<unsigned long long>()); break;
+                default: gx::k_digit_hist<<<g, 256, sh, cs(s)>>>(k.as<uint64_t>(), k.n, b, mask, P, counts.get<unsigned long long>()); break;
+            }
+            GX_LAUNCHED();
         }
-        GX_LAUNCHED();
+        gx::exclusive_scan_i64(counts.get<int64_t>(), ex.get<int64_t>(), P, cs(s));
+        GX_CUDA(cudaMemcpyAsync(o.buf.get<int64_t>(), ex.get<int64_t>() + 1, (size_t)P * 8, cudaMemcpyDeviceToDevice, cs(s)));
+        GX_CUDA(cudaMemcpyAsync(o.buf.get<int64_t>() + P, ex.get<int64_t>() + P, 8, cudaMemcpyDeviceToDevice, cs(s)));
         GX_CUDA(cudaStreamSynchronize(cs(s)));
         *out = gx::to_gx_column(std::move(o));
     })

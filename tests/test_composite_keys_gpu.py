@@ -191,12 +191,21 @@ def test_multikey_compress_equality_and_bits():
     assert bits == 3 + 6
     f = fused.cpu().numpy().view(np.uint64)
     pairs = a.astype(np.int64) * 1000 + b
-    # equal fused keys <=> equal key rows
-    assert len(np.unique(f)) == len(np.unique(pairs))
-    assert np.array_equal(np.unique(f, return_inverse=True)[1], np.unique(pairs, return_inverse=True)[1])
+    # equal fused keys <=> equal key rows: fused key <-> key row is a bijection
+    both = set(zip(f.tolist(), pairs.tolist()))
+    assert len(both) == len(set(f.tolist())) == len(set(pairs.tolist()))
     assert gx.multikey_compress([to_dev(a), to_dev(np.zeros(n, np.float32))]) is None
+    # Wide-range columns fall back to dictionary codes: 50000 distinct values
+    # take 16 bits each.
     wide = rng.integers(-2**62, 2**62, size=n, dtype=np.int64)
-    assert gx.multikey_compress([to_dev(wide), to_dev(wide)], max_bits=64) is None
+    fused, bits = gx.multikey_compress([to_dev(wide), to_dev(wide[::-1].copy())])
+    assert bits == 32
+    f = fused.cpu().numpy().view(np.uint64)
+    assert len(set(zip(f.tolist(), wide.tolist(), wide[::-1].tolist()))) == len(set(f.tolist())) == n
+    # Three columns of ~2^22 distinct values need 3 x 23 bits: more than 64.
+    m = 1 << 22
+    cols = [to_dev(rng.integers(-2**62, 2**62, size=m, dtype=np.int64)) for _ in range(3)]
+    assert gx.multikey_compress(cols, max_bits=64) is None
 
 
 def test_gather_numeric_and_strings():
