@@ -84,10 +84,12 @@ __device__ __forceinline__ void g_update(uint64_t* r, const agg_desc& d, const u
 }
 
 // Shared-memory table of one CTA:
-//   keys[S] (u32 or u64) | counts[R][S] (u32) | acc[R][A][S] (u64)
+//   keys[S] (u32 or u64) | counts[S][R] (u32) | acc[A][S][R] (u64)
 // The key table is shared by the CTA; the accumulators are replicated R
-// times (warp w updates replica w % R) so that low-cardinality inputs do not
-// serialise on a handful of shared-memory words.
+// times (thread t updates replica t % R) so that low-cardinality inputs do
+// not serialise on a handful of shared-memory words.  Replicas are the
+// innermost index: with R = 32 the lanes of a warp update 32 different
+// banks whatever slots they hit (R = 16: conflict-free 8-byte updates).
 template <int KW>
 struct stable {
     using kt = typename std::conditional<KW == 4, uint32_t, unsigned long long>::type;
@@ -159,18 +161,17 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restri
         const kt EMPTY = KW == 4 ? (kt)S_EMPTY4 : (kt)S_EMPTY8;
         for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) st.keys[i] = EMPTY;
         for (uint32_t i = threadIdx.x; i < s_slots * reps; i += HGB_NT) st.counts[i] = 0;
-        for (int r = 0; r < reps; ++r)
-            for (int a = 0; a < d.n_acc; ++a) {
-                uint64_t idv = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
-                uint64_t* base = st.acc + ((size_t)r * d.n_acc + a) * S;
-                for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) base[i] = idv;
-            }
+        for (int a = 0; a < d.n_acc; ++a) {
+            uint64_t idv = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
+            uint64_t* base = st.acc + (size_t)a * S * reps;
+            for (uint32_t i = threadIdx.x; i < s_slots * reps; i += HGB_NT) base[i] = idv;
+        }
         if (threadIdx.x == 0) s_fill = 0;
         // Spread a warp's lanes over the replicas: lanes of one warp that hit
         // the same group then update different words.
         const int rep = (int)(threadIdx.x % (unsigned)reps);
-        my_counts = st.counts + (size_t)rep * S;
-        my_acc = st.acc + (size_t)rep * d.n_acc * S;
+        my_counts = st.counts + rep;
+        my_acc = st.acc + rep;
         __syncthreads();
     }
 
@@ -218,9 +219,9 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restri
                 if (valid && slot >= 0) {
                     // The per-replica count is kept even without COUNT: it
                     // tells the merge which replicas saw the group (for ANY).
-                    atomicAdd(&my_counts[slot], 1u);
-                    if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, slot, v[u]);
-                    else dev_::shared_row_update<NV>(my_acc, s_slots, slot, d, v[u]);
+                    atomicAdd(&my_counts[slot * reps], 1u);
+                    if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots * reps, slot * reps, v[u]);
+                    else dev_::shared_row_update<NV>(my_acc, (size_t)s_slots * reps, slot * reps, d, v[u]);
                 }
             }
             __syncwarp();
@@ -247,9 +248,9 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restri
                 __syncwarp();
                 if (live) {
                     if (sq >= 0) {
-                        atomicAdd(&my_counts[sq], 1u);
-                        if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, sq, vq);
-                        else dev_::shared_row_update<NV>(my_acc, s_slots, sq, d, vq);
+                        atomicAdd(&my_counts[sq * reps], 1u);
+                        if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots * reps, sq * reps, vq);
+                        else dev_::shared_row_update<NV>(my_acc, (size_t)s_slots * reps, sq * reps, d, vq);
                     } else {
                         uint64_t* r = g_find_or_insert<KW>(g, d, kq, hq);
                         if (r) g_update(r, d, vq, 1ull);
@@ -281,18 +282,18 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restri
             unsigned long long c = 0;
             int first = -1;
             for (int rp = 0; rp < reps; ++rp) {
-                unsigned cr = st.counts[(size_t)rp * s_slots + i];
+                unsigned cr = st.counts[(size_t)i * reps + rp];
                 c += cr;
                 if (cr && first < 0) first = rp;
             }
             if (first < 0) continue;
             if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), c);
             for (int a = 0; a < d.n_acc; ++a) {
-                uint64_t x = st.acc[((size_t)first * d.n_acc + a) * s_slots + i];
+                uint64_t x = st.acc[((size_t)a * s_slots + i) * reps + first];
                 for (int rp = first + 1; rp < reps; ++rp)
-                    if (st.counts[(size_t)rp * s_slots + i])
+                    if (st.counts[(size_t)i * reps + rp])
                         x = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], x,
-                                              st.acc[((size_t)rp * d.n_acc + a) * s_slots + i]);
+                                              st.acc[((size_t)a * s_slots + i) * reps + rp]);
                 dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], x);
             }
         }
@@ -339,19 +340,18 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
     st.S = s_slots;
     st.R = reps;
     const int rep = (int)(threadIdx.x % (unsigned)reps);
-    unsigned* my_counts = st.counts + (size_t)rep * S;
-    uint64_t* my_acc = st.acc + (size_t)rep * d.n_acc * S;
+    unsigned* my_counts = st.counts + rep;
+    uint64_t* my_acc = st.acc + rep;
     const int64_t nu = *n_units;
     for (int64_t u = blockIdx.x; u < nu; u += gridDim.x) {
         const part_unit un = units[u];
         for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) st.keys[i] = EMPTY;
         for (uint32_t i = threadIdx.x; i < s_slots * reps; i += HGB_NT) st.counts[i] = 0;
-        for (int r = 0; r < reps; ++r)
-            for (int a = 0; a < d.n_acc; ++a) {
-                const uint64_t idv = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
-                uint64_t* base = st.acc + ((size_t)r * d.n_acc + a) * S;
-                for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) base[i] = idv;
-            }
+        for (int a = 0; a < d.n_acc; ++a) {
+            const uint64_t idv = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
+            uint64_t* base = st.acc + (size_t)a * S * reps;
+            for (uint32_t i = threadIdx.x; i < s_slots * reps; i += HGB_NT) base[i] = idv;
+        }
         if (threadIdx.x == 0) { s_fill = 0; s_spill = 0; }
         __syncthreads();
         const int64_t tile = (int64_t)HGB_NT * HU_UNROLL;
@@ -377,9 +377,9 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
             __syncwarp();  // regroup after the probe loop (see k_hash_groupby)
             if (!live) return;
             if (sq >= 0) {
-                atomicAdd(&my_counts[sq], 1u);
-                if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, sq, vq);
-                else dev_::shared_row_update<NV>(my_acc, s_slots, sq, d, vq);
+                atomicAdd(&my_counts[sq * reps], 1u);
+                if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots * reps, sq * reps, vq);
+                else dev_::shared_row_update<NV>(my_acc, (size_t)s_slots * reps, sq * reps, d, vq);
             } else {
                 if (!s_spill) s_spill = 1;
                 uint64_t* r = g_find_or_insert<KW>(g, d, kq, hq);
@@ -435,9 +435,9 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
                 if (miss) s_q[warp][qfill + __popc(mm & lt)] = (uint32_t)(i - un.begin);
                 qfill += __popc(mm);
                 if (valid && slot[q] >= 0) {
-                    atomicAdd(&my_counts[slot[q]], 1u);
-                    if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots, slot[q], v[q]);
-                    else dev_::shared_row_update<NV>(my_acc, s_slots, slot[q], d, v[q]);
+                    atomicAdd(&my_counts[slot[q] * reps], 1u);
+                    if constexpr (sizeof...(ACCS) > 0) spec::apply_all<0, ACCS...>(my_acc, s_slots * reps, slot[q] * reps, v[q]);
+                    else dev_::shared_row_update<NV>(my_acc, (size_t)s_slots * reps, slot[q] * reps, d, v[q]);
                 }
             }
             __syncwarp();
@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
                     unsigned long long c = 0;
                     int first = -1;
                     for (int rp = 0; rp < reps; ++rp) {
-                        const unsigned cr = st.counts[(size_t)rp * S + i];
+                        const unsigned cr = st.counts[(size_t)i * reps + rp];
                         c += cr;
                         if (cr && first < 0) first = rp;
                     }
@@ -479,11 +479,11 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
                     for (int a = 0; a < d.n_acc; ++a) {
                         uint64_t x = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
                         if (first >= 0) {
-                            x = st.acc[((size_t)first * d.n_acc + a) * S + i];
+                            x = st.acc[((size_t)a * S + i) * reps + first];
                             for (int rp = first + 1; rp < reps; ++rp)
-                                if (st.counts[(size_t)rp * S + i])
+                                if (st.counts[(size_t)i * reps + rp])
                                     x = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], x,
-                                                          st.acc[((size_t)rp * d.n_acc + a) * S + i]);
+                                                          st.acc[((size_t)a * S + i) * reps + rp]);
                         }
                         r[d.acc_word0 + a] = x;
                     }
@@ -500,18 +500,18 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
                 unsigned long long c = 0;
                 int first = -1;
                 for (int rp = 0; rp < reps; ++rp) {
-                    const unsigned cr = st.counts[(size_t)rp * S + i];
+                    const unsigned cr = st.counts[(size_t)i * reps + rp];
                     c += cr;
                     if (cr && first < 0) first = rp;
                 }
                 if (first < 0) continue;
                 if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), c);
                 for (int a = 0; a < d.n_acc; ++a) {
-                    uint64_t x = st.acc[((size_t)first * d.n_acc + a) * S + i];
+                    uint64_t x = st.acc[((size_t)a * S + i) * reps + first];
                     for (int rp = first + 1; rp < reps; ++rp)
-                        if (st.counts[(size_t)rp * S + i])
+                        if (st.counts[(size_t)i * reps + rp])
                             x = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], x,
-                                                  st.acc[((size_t)rp * d.n_acc + a) * S + i]);
+                                                  st.acc[((size_t)a * S + i) * reps + rp]);
                     dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], x);
                 }
             }
@@ -562,6 +562,9 @@ int hash_smem_slots(const agg_desc& d, int key_width, int64_t groups_bound, int*
     size_t r = (budget - (size_t)s * key_width) / ((size_t)s * per_rep);
     if (r < 1) r = 1;
     if (r > 32) r = 32;
+    // A power of two: with replicas innermost, lanes then spread evenly over
+    // the banks.
+    while (r & (r - 1)) r &= r - 1;
     *replicas = (int)r;
     return (int)s;
 }
@@ -774,6 +777,7 @@ bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d,
     if ((size_t)slots * (kw + per_rep) > budget) return false;
     size_t reps = (budget - (size_t)slots * kw) / ((size_t)slots * per_rep);
     reps = std::max<size_t>(1, std::min<size_t>(32, reps));
+    while (reps & (reps - 1)) reps &= reps - 1;
     const size_t smem = (((size_t)slots * kw + 15) & ~size_t(15)) + (((size_t)slots * 4 * reps + 15) & ~size_t(15)) +
                         (size_t)slots * reps * 8 * d.n_acc;
     units_args a{keys, kind, units, n_units, slots, (int)reps, shift,
