@@ -91,3 +91,77 @@ def test_split_requests_rewrites_avg_and_count():
     assert finals == [(AVG, [1, 2]), (COUNT_ALL, [3]), (MAX, [4])]
     with pytest.raises(ValueError):
         split_requests([(0, 99)])
+
+
+NB, NP = 3_000, 20_000
+
+
+def join_data():
+    import oracle as O
+    bk = O.gen_keys(NB, np.int32, seed=7, groups=2_000)          # duplicate build keys
+    pk = O.gen_keys(NP, np.int32, seed=8, groups=2_500)          # some probe keys absent
+    return bk, pk
+
+
+def oracle_join(bk, pk):
+    import torch
+    import oracle as O
+    l, r = O.join_pairs(bk.numpy(), pk.numpy())
+    return torch.from_numpy(l), torch.from_numpy(r)
+
+
+def join_worker(rank, rdv, strategy, failures):
+    import torch
+    import torch.distributed as dist
+    import oracle as O
+    from eiger_b200.distributed import distributed_join
+    try:
+        dist.init_process_group("gloo", init_method=f"file://{rdv}", rank=rank, world_size=WORLD)
+        bk, pk = join_data()
+        blo, bhi = rank * NB // WORLD, (rank + 1) * NB // WORLD
+        plo, phi = (rank * NP) // 3, ((rank + 1) * NP) // 3 if rank + 1 < WORLD else NP  # uneven shards
+        b, p = distributed_join(torch.from_numpy(bk[blo:bhi].copy()), torch.from_numpy(pk[plo:phi].copy()), blo, plo,
+                                strategy=strategy, local_join=oracle_join)
+        # gather every rank's pairs on every rank and compare with the oracle
+        n = torch.tensor([b.numel()], dtype=torch.int64)
+        sizes = [torch.zeros_like(n) for _ in range(WORLD)]
+        dist.all_gather(sizes, n)
+        m = max(int(s.item()) for s in sizes)
+        bb = torch.full((m,), -1, dtype=torch.int64)
+        pp = torch.full((m,), -1, dtype=torch.int64)
+        bb[: b.numel()], pp[: p.numel()] = b, p
+        ab = [torch.empty_like(bb) for _ in range(WORLD)]
+        ap = [torch.empty_like(pp) for _ in range(WORLD)]
+        dist.all_gather(ab, bb)
+        dist.all_gather(ap, pp)
+        gb = torch.cat([x[: int(s.item())] for x, s in zip(ab, sizes)]).numpy()
+        gp = torch.cat([x[: int(s.item())] for x, s in zip(ap, sizes)]).numpy()
+        o = np.lexsort((gp, gb))
+        el, er = O.join_pairs(bk, pk)
+        assert np.array_equal(gb[o], el) and np.array_equal(gp[o], er)
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as e:
+        failures.put(f"rank {rank}: {type(e).__name__}: {e}")
+        raise
+
+
+@pytest.mark.parametrize("strategy", ["broadcast", "shuffle"])
+def test_two_rank_join_matches_single_oracle(strategy):
+    ctx = mp.get_context("spawn")
+    failures = ctx.SimpleQueue()
+    with tempfile.TemporaryDirectory() as d:
+        rdv = os.path.join(d, "rdv")
+        procs = [ctx.Process(target=join_worker, args=(r, rdv, strategy, failures)) for r in range(WORLD)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+        for p in procs:
+            if p.is_alive():
+                p.kill()
+    msgs = []
+    while not failures.empty():
+        msgs.append(failures.get())
+    assert not msgs, msgs
+    assert all(p.exitcode == 0 for p in procs)
