@@ -169,6 +169,7 @@ def _load() -> C.CDLL:
         "gx_profile_reset": ([], None),
         "gx_profile_read": ([C.c_char_p, C.POINTER(C.c_double), C.POINTER(i64)], i32),
         "gx_selector_features": ([cv, vp, vp], i32),
+        "gx_selector_plan_features": ([tv, C.POINTER(AggRequest), i32, i32, vp], i32),
         "gx_selector_param_count": ([], i64),
         "gx_selector_load": ([vp, vp, vp], i32),
         "gx_selector_predict": ([vp, i32, vp], i32),

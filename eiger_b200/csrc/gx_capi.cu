@@ -34,6 +34,7 @@ void radix_sort_biased(const col& keys_c, const void* vals_in, int val_width, bo
 void generate_strings(const char* dchars, const int64_t* doff, int64_t dsize, const int32_t* codes, int64_t rows,
                       const int64_t* off, char* out, cudaStream_t s);
 void selector_features(const col& key, float* f, cudaStream_t s);
+void selector_plan_features(const agg_plan& p, float* f4);
 int64_t selector_param_count();
 void selector_load(const uint16_t* params, const float* mean, const float* stdv);
 void selector_predict(const float* feats, int rows, float* scores, cudaStream_t s);
@@ -468,6 +469,14 @@ gx_status gx_compute_min_max(gx_column_view c, gx_stream_t s, void* mn, void* mx
     GX_TRY({
         gx::require(mn && mx, "null output");
         gx::compute_min_max(resolve(c), mn, mx, cs(s));
+    })
+}
+
+gx_status gx_selector_plan_features(const gx_table_view* val, const gx_agg_request* req, int32_t n, int32_t agg_count,
+                                    float* out4) {
+    GX_TRY({
+        gx::require(out4 != nullptr, "null output");
+        gx::selector_plan_features(gx::make_agg_plan(val, req, n, agg_count != 0), out4);
     })
 }
 

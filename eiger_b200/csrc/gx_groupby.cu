@@ -15,9 +15,10 @@ namespace gx {
 
 // Learned selector (gx_selector.cu): returns the variant (gx_groupby_algo)
 // and writes the suggested radix bits.
-int selector_choose(const col& key, int* radix_bits, cudaStream_t s);
+int selector_choose(const col& key, const agg_plan& plan, int* radix_bits, cudaStream_t s);
 
-static void auto_select(const gx_table_view* key, gx_groupby_hint* hint, cudaStream_t s) {
+static void auto_select(const gx_table_view* key, const gx_table_view* val, const gx_agg_request* req, int nreq,
+                        gx_groupby_hint* hint, cudaStream_t s) {
     if (hint->groupby_algo != GX_GB_AUTO) return;
     for (int64_t i = 0; i < key->num_columns; ++i)
         if (key->columns[i].type == GX_STRING) { hint->groupby_algo = GX_GB_HASH; return; }
@@ -25,7 +26,8 @@ static void auto_select(const gx_table_view* key, gx_groupby_hint* hint, cudaStr
     col k = resolve(key->columns[0]);
     if (hint->selector == GX_SELECT_LEARNED) {
         int bits = 0;
-        hint->groupby_algo = selector_choose(k, &bits, s);
+        const agg_plan plan = make_agg_plan(val, req, nreq, hint->agg_count != 0);
+        hint->groupby_algo = selector_choose(k, plan, &bits, s);
         if (hint->radix_bits <= 0) hint->radix_bits = bits;
         return;
     }
@@ -106,7 +108,7 @@ void groupby_dispatch(const gx_table_view* key, const gx_table_view* val, const 
                                                    " has a different row count than the key");
 
     if (forced_algo >= 0) hint->groupby_algo = forced_algo;
-    auto_select(key, hint, s);
+    auto_select(key, val, req, nreq, hint, s);
     bool str = false;
     for (int64_t i = 0; i < key->num_columns; ++i) str |= key->columns[i].type == GX_STRING;
     const bool composite = str || key->num_columns > 1;

@@ -748,7 +748,7 @@ void hash_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hint, c
         // 2^28 rows; uniform keys: 16.6 ms without, 21.7 ms with).  Switch it
         // on when the 8 most frequent keys of a 2^14-row sample carry >= 5%
         // of the sample.
-        float f[16];
+        float f[GX_SEL_NUM_FEATURES];
         selector_features(key, f, s);
         float top = 0.f;
         for (int t = 0; t < 8; ++t) top += f[6 + t];

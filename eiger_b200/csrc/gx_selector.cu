@@ -8,9 +8,10 @@
 // fraction, top-8 key frequencies, a GEE extrapolation of the distinct count
 // — Charikar, Chaudhuri, Motwani, Narasayya, PODS 2000) and scores the
 // HASH / SORT / PARTITION variants and four partition fan-outs with a
-// 3-layer MLP (16 -> 64 -> 64 -> 7, ReLU) whose weights are stored in FP16
-// and whose arithmetic accumulates in FP32.  Training runs on the GPU with
-// the forward / backward / Adam kernels below.
+// 3-layer MLP (20 -> 64 -> 64 -> 7, ReLU) whose weights are stored in FP16
+// and whose arithmetic accumulates in FP32; 4 of its 20 inputs describe the
+// aggregation list.  Training runs on the GPU with the forward / backward /
+// Adam kernels below.
 #include <algorithm>
 #include <cmath>
 #include <cuda_fp16.h>
@@ -154,6 +155,17 @@ selector_state g_sel;
 
 }  // namespace
 
+// Features 16..19: the aggregation list (cost drivers of every variant's
+// per-row work): value bytes read per row, accumulators, float SUMs (64-bit
+// shared-memory adds are emulated, several times a 32-bit atomic) and
+// MIN / MAX accumulators.
+void selector_plan_features(const agg_plan& p, float* f4) {
+    f4[0] = (float)((double)p.value_bytes_per_row / 32.0);
+    f4[1] = (float)(p.d.n_acc / 8.0);
+    f4[2] = (float)(p.d.n_cls[CL_FSUM] / 4.0);
+    f4[3] = (float)((p.d.n_cls[CL_MIN] + p.d.n_cls[CL_MAX]) / 8.0);
+}
+
 void selector_features(const col& key_in, float* f, cudaStream_t s) {
     owned_col widened;
     col key = key_in;
@@ -281,7 +293,7 @@ void selector_predict(const float* feats, int rows, float* scores, cudaStream_t 
 
 // AUTO with the learned selector; falls back to the reference's NDV rule
 // when no weights are loaded.
-int selector_choose(const col& key, int* radix_bits, cudaStream_t s) {
+int selector_choose(const col& key, const agg_plan& plan, int* radix_bits, cudaStream_t s) {
     *radix_bits = 0;
     if (!selector_loaded()) {
         int64_t est = ndv_estimate(key, s);
@@ -289,6 +301,7 @@ int selector_choose(const col& key, int* radix_bits, cudaStream_t s) {
     }
     float f[F], y[O];
     selector_features(key, f, s);
+    selector_plan_features(plan, f + GX_SEL_KEY_FEATURES);
     selector_predict(f, 1, y, s);
     static const int variants[3] = {GX_GB_HASH, GX_GB_SORT, GX_GB_PARTITION};
     int best = 0;

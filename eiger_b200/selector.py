@@ -23,7 +23,8 @@ from pathlib import Path
 
 import numpy as np
 
-F, H, O = 16, 64, 7
+F, H, O = 20, 64, 7
+KF = 16              # key-sample features; the last 4 describe the aggregation list
 NV = 3               # variants: HASH, SORT, PARTITION
 FANOUTS = [8, 10, 12, 14]
 WEIGHTS = Path(__file__).resolve().parent / "selector_weights.npz"
@@ -40,8 +41,12 @@ def param_count() -> int:
 
 # ---------------------------------------------------------------------------
 # Instances (C4: rows log-uniform in 2^16..2^28, NDV log-uniform in 1..rows,
-# Zipf s uniform in [0, 2], int32 or int64 keys; SUM + COUNT of int64 values)
+# Zipf s uniform in [0, 2], int32 or int64 keys).  Half the instances run
+# SUM + COUNT of an int64 column, half SUM / MIN / MAX of an int64 and a
+# float64 column plus COUNT (the benchmark's aggregation list).
 # ---------------------------------------------------------------------------
+AGGS = {"sumcount": [(0, 0), (0, 5)],
+        "seven": [(0, 0), (0, 2), (0, 1), (1, 0), (1, 2), (1, 1), (0, 5)]}  # (column, gx agg kind)
 def draw_instances(count: int, seed: int, min_log2=16, max_log2=28) -> list[dict]:
     rng = np.random.default_rng(seed)
     out = []
@@ -49,7 +54,8 @@ def draw_instances(count: int, seed: int, min_log2=16, max_log2=28) -> list[dict
         rows = int(2 ** rng.uniform(min_log2, max_log2))
         ndv = int(max(1, round(2 ** rng.uniform(0, math.log2(rows)))))
         out.append({"rows": rows, "ndv": ndv, "zipf": float(rng.uniform(0, 2)),
-                    "key": "int64" if rng.random() < 0.5 else "int32", "seed": int(seed * 100003 + i)})
+                    "key": "int64" if rng.random() < 0.5 else "int32", "seed": int(seed * 100003 + i),
+                    "aggs": "seven" if rng.random() < 0.5 else "sumcount"})
     return out
 
 
@@ -69,13 +75,30 @@ def make_instance(inst: dict):
     gx.generate_keys(k, spec)
     v = torch.empty(rows, dtype=torch.int64, device="cuda")
     gx.generate_values(v, gx.gen_spec(seed=inst["seed"], stream_id=1, lo=0, hi=1 << 31))
-    return k, v, cdf
+    vals = [v]
+    if inst.get("aggs", "sumcount") == "seven":
+        f = torch.empty(rows, dtype=torch.float64, device="cuda")
+        gx.generate_values(f, gx.gen_spec(seed=inst["seed"], stream_id=2))
+        vals.append(f)
+    return k, vals, cdf
 
 
-def features(key) -> np.ndarray:
+def plan_features(vals, reqs) -> np.ndarray:
+    """Features 16..19 (the aggregation list), computed by the library."""
+    gx = _gx()
+    tv, _keep = gx.table_view(vals)
+    arr = (gx.AggRequest * len(reqs))(*[gx.AggRequest(c, k) for c, k in reqs])
+    out = np.zeros(F - KF, dtype=np.float32)
+    gx.check(gx.lib.gx_selector_plan_features(C.byref(tv), arr, len(reqs), 0, out.ctypes.data))
+    return out
+
+
+def features(key, vals=None, reqs=None) -> np.ndarray:
     gx = _gx()
     f = np.zeros(F, dtype=np.float32)
     gx.check(gx.lib.gx_selector_features(gx.view(key), gx._stream_ptr(None), f.ctypes.data))
+    if vals is not None:
+        f[KF:] = plan_features(vals, reqs)
     return f
 
 
@@ -118,7 +141,6 @@ def collect(instances: list[dict], start: int = 0, count: int | None = None, fan
     import torch
     gx = _gx()
     log = log or (lambda m: print(m, flush=True))
-    reqs = [(0, gx.SUM), (0, gx.COUNT_ALL)]
     stop = len(instances) if count is None else min(len(instances), start + count)
     index, feats, times, ftimes, heur = [], [], [], [], []
     phase = {"make": 0.0, "features": 0.0, "variants": 0.0, "fanouts": 0.0, "heuristic": 0.0}
@@ -137,21 +159,22 @@ def collect(instances: list[dict], start: int = 0, count: int | None = None, fan
             Path(str(out) + ".progress").write_text(f"{idx} start\n")
         t0 = time.perf_counter()
         k, v, cdf = make_instance(inst)
+        reqs = AGGS[inst.get("aggs", "sumcount")]
         t0 = clock("make", t0)
-        f = features(k)
+        f = features(k, v, reqs)
         t0 = clock("features", t0)
         row = []
         for algo in (gx.HASH, gx.SORT, gx.PARTITION):
             if out:
                 Path(str(out) + ".progress").write_text(f"{idx} variant {algo}\n")
-            row.append(time_call(lambda: gx.groupby([k], [v], reqs, gx.make_hint(algo))))
+            row.append(time_call(lambda: gx.groupby([k], v, reqs, gx.make_hint(algo))))
         t0 = clock("variants", t0)
         fr = [np.nan] * len(FANOUTS)
         if idx % fanout_every == 0:
             for j, bits in enumerate(FANOUTS):
                 if out:
                     Path(str(out) + ".progress").write_text(f"{idx} fanout {bits}\n")
-                fr[j] = time_call(lambda: gx.groupby([k], [v], reqs, gx.make_hint(gx.PARTITION, radix_bits=bits)))
+                fr[j] = time_call(lambda: gx.groupby([k], v, reqs, gx.make_hint(gx.PARTITION, radix_bits=bits)))
         t0 = clock("fanouts", t0)
         h = heuristic_algo(k)
         clock("heuristic", t0)
@@ -258,6 +281,8 @@ def install(path: Path | None = None) -> bool:
         return False
     d = np.load(path)
     p = np.ascontiguousarray(d["params"], np.uint16)
+    if p.size != param_count() or d["mean"].size != F:
+        return False  # weights of another network shape: keep the plain rule
     mean = np.ascontiguousarray(d["mean"], np.float32)
     std = np.ascontiguousarray(d["std"], np.float32)
     gx.check(gx.lib.gx_selector_load(p.ctypes.data, mean.ctypes.data, std.ctypes.data))
@@ -302,10 +327,25 @@ def main() -> None:
     learned = np.argmin(y[:, :NV], axis=1)
     heur = heuristic_choice(d["heuristic"][ntr:])
     oracle_best = np.argmin(times[ntr:], axis=1)
+    # Fan-out head: on held-out instances with measured fan-outs, the chosen
+    # radix bits against the best of the four, beside a fixed 8 bits (one
+    # radix pass, what the engine defaults to near 2^16 groups).
+    fth = ft[ntr:]
+    fok = ~np.isnan(fth).any(axis=1)
+    fchoice = np.argmin(y[fok][:, NV:], axis=1)
+    insts = json.loads(str(d["instances"]))[ntr:]
+    kinds = np.array([i.get("aggs", "sumcount") for i in insts])
     report = {"train_instances": int(ntr), "heldout_instances": int(n - ntr),
               "regret_learned": regret(times[ntr:], learned), "regret_heuristic": regret(times[ntr:], heur),
               "accuracy_learned": float(np.mean(learned == oracle_best)),
               "accuracy_heuristic": float(np.mean(heur == oracle_best)),
+              "regret_learned_by_aggs": {k: regret(times[ntr:][kinds == k], learned[kinds == k])
+                                         for k in AGGS if (kinds == k).any()},
+              "regret_heuristic_by_aggs": {k: regret(times[ntr:][kinds == k], heur[kinds == k])
+                                           for k in AGGS if (kinds == k).any()},
+              "fanout_instances": int(fok.sum()),
+              "fanout_regret_learned": regret(fth[fok], fchoice) if fok.any() else None,
+              "fanout_regret_fixed_8_bits": regret(fth[fok], np.zeros(int(fok.sum()), np.int64)) if fok.any() else None,
               "loss_history": hist,
               "best_variant_share": np.bincount(oracle_best, minlength=NV).tolist()}
     save(Path(a.out), params, mean, std, report)
@@ -313,7 +353,8 @@ def main() -> None:
     if a.report:
         Path(a.report).write_text(json.dumps(report, indent=1))
     if a.heldout_out:
-        np.savez(a.heldout_out, features=x[ntr:], times=times[ntr:], heuristic=d["heuristic"][ntr:])
+        np.savez(a.heldout_out, features=x[ntr:], times=times[ntr:], heuristic=d["heuristic"][ntr:],
+                 fanout_times=ft[ntr:], aggs=np.array([i.get("aggs", "sumcount") for i in insts]))
 
 
 if __name__ == "__main__":

@@ -506,7 +506,8 @@ gx_status gx_fill_sequence(gx_column_view out, int64_t start, int64_t step,
 /* ---------------------------------------------------------------------- */
 /* Learned strategy selector.                                              */
 /* ---------------------------------------------------------------------- */
-#define GX_SEL_NUM_FEATURES 16
+#define GX_SEL_NUM_FEATURES 20   /* 16 key-sample features + 4 of the aggregation list */
+#define GX_SEL_KEY_FEATURES 16
 #define GX_SEL_HIDDEN 64
 #define GX_SEL_NUM_VARIANTS 3   /* 0 = HASH, 1 = SORT, 2 = PARTITION */
 #define GX_SEL_NUM_FANOUTS 4    /* radix bits {8, 10, 12, 14} */
@@ -515,8 +516,14 @@ gx_status gx_fill_sequence(gx_column_view out, int64_t start, int64_t step,
 
 /* Sketch of a 2^14-row strided sample of a key column: HLL distinct
  * estimate of the sample, top-8 key frequencies, rows/distinct ratio,
- * dtype and log-size terms, written as GX_SEL_NUM_FEATURES floats. */
+ * dtype and log-size terms: features 0..15 of GX_SEL_NUM_FEATURES floats
+ * (16..19 are written as zero; see gx_selector_plan_features). */
 gx_status gx_selector_features(gx_column_view key, gx_stream_t stream, float* features_host);
+/* Features 16..19 (written to out4[0..3]): the aggregation list the group-by
+ * will run — value bytes read per row / 32, accumulators / 8, float SUM
+ * accumulators / 4, MIN and MAX accumulators / 8 — as AUTO sees them. */
+gx_status gx_selector_plan_features(const gx_table_view* val, const gx_agg_request* requests,
+                                    int32_t num_requests, int32_t agg_count, float* out4);
 /* Number of fp16 parameters of the 3-layer MLP. */
 int64_t gx_selector_param_count(void);
 /* Install trained fp16 weights (host array of gx_selector_param_count halves). */

@@ -1,8 +1,8 @@
 """NumPy restatement of the selector MLP — TEST INFRASTRUCTURE ONLY.
 
-Float64 forward and backward of the 16 -> 64 -> 64 -> 7 ReLU network whose
+Float64 forward and backward of the 20 -> 64 -> 64 -> 7 ReLU network whose
 FP16 parameters the library's selector kernels use (parameter layout:
-W1[64][16], b1[64], W2[64][64], b2[64], W3[7][64], b3[7]), with the same
+W1[64][20], b1[64], W2[64][64], b2[64], W3[7][64], b3[7]), with the same
 masked mean-squared-error loss, mean over rows x outputs.  The selector has
 no counterpart in the reference; this is the checker for the device
 gradients.
@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import numpy as np
 
-F, H, O = 16, 64, 7
+F, H, O = 20, 64, 7
 SIZES = [("W1", (H, F)), ("b1", (H,)), ("W2", (H, H)), ("b2", (H,)), ("W3", (O, H)), ("b3", (O,))]
 TOTAL = sum(int(np.prod(s)) for _, s in SIZES)
 

@@ -57,3 +57,34 @@ def test_report_matches_recomputation(data):
     # the GPU forward (FP16 weights, FP32 accumulation) and this float64 one
     # may split a near-tie differently on a few instances
     assert abs(regret(h["times"], learned) - meta["regret_learned"]) < 0.02
+
+
+def test_fanout_head_beats_a_fixed_fanout(data):
+    # Outputs 3..6 score PARTITION at 8 / 10 / 12 / 14 radix bits; on the
+    # held-out instances whose fan-outs were all timed, the chosen bits must
+    # cost less than always taking one 8-bit pass.
+    w, h = data
+    if "fanout_times" not in h.files:
+        pytest.skip("held-out set without fan-out timings")
+    ft = h["fanout_times"]
+    ok = ~np.isnan(ft).any(axis=1)
+    params = w["params"].view(np.float16).astype(np.float64)
+    x = (h["features"][ok] - w["mean"]) / w["std"]
+    choice = np.argmin(M.forward(params, x)[:, 3:], axis=1)
+    assert ok.sum() >= 100
+    assert regret(ft[ok], choice) < regret(ft[ok], np.zeros(int(ok.sum()), np.int64))
+
+
+def test_both_aggregation_lists_are_covered(data):
+    # Half the instances run SUM + COUNT, half the 7-aggregate list of the
+    # benchmark; the learned choice stays within 10% regret on each.
+    w, h = data
+    if "aggs" not in h.files:
+        pytest.skip("held-out set without the aggregation list")
+    params = w["params"].view(np.float16).astype(np.float64)
+    x = (h["features"] - w["mean"]) / w["std"]
+    learned = np.argmin(M.forward(params, x)[:, :3], axis=1)
+    for kind in ("sumcount", "seven"):
+        m = h["aggs"] == kind
+        assert m.sum() >= 300
+        assert regret(h["times"][m], learned[m]) <= 0.10
