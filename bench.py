@@ -339,6 +339,13 @@ def run_gx(args) -> None:
             join["cpu_baseline"] = cpu_join_baseline(bk.cpu().numpy(), pk.cpu().numpy())
         del bk, brow, pk, prow
 
+    # ------------------------------------------------------- sweep grid
+    # The group-by sweep at the timed row count, every variant: G over the
+    # sweep's range (int32 keys, uniform), plus Zipf 1.5 and int64 keys.
+    sweep = None
+    if not args.no_sweep:
+        sweep = sweep_grid(gx, torch, rows, peaks, dist)
+
     # ----------------------------------------------------------- batched
     batched = None
     if args.batch_instances > 0:
@@ -387,12 +394,50 @@ def run_gx(args) -> None:
                        "selector": "learned" if learned else ("plain" if args.algo == "auto" else "forced"),
                        "l2": "inputs (5.4 GB) larger than L2; no flush"},
             "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk.summary(), "join": join, "batched": batched,
+            "clocks": clk.summary(), "join": join, "batched": batched, "sweep": sweep,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def sweep_grid(gx, torch, rows: int, peaks: dict, dist=None) -> list:
+    """HASH / SORT / PARTITION over a grid of group counts and skews, 7
+    aggregates, at `rows` rows: ms, Grows/s and fraction of measured HBM per
+    point (algorithmic bytes rows * (K + 16) + groups * (K + 56))."""
+    reqs = groupby_reqs(gx)
+    points = [("int32", 0.0, 1 << g) for g in (4, 10, 16, 20, 24, 26)]
+    points += [("int32", 1.5, 1 << 20), ("int64", 0.0, 1 << 16), ("int64", 1.5, 1 << 24)]
+    out = []
+    for kdt, z, G in points:
+        k = torch.empty(rows, dtype=torch.int32 if kdt == "int32" else torch.int64, device="cuda")
+        cdf = None
+        if z > 0:
+            cdf = torch.from_numpy(gx.zipf_cdf(G, z)).cuda()
+            spec = gx.gen_spec(seed=1, dist=gx.DIST_ZIPF, groups=G, zipf_s=z, scatter=1, zipf_cdf=cdf.data_ptr())
+        else:
+            spec = gx.gen_spec(seed=1, groups=G, scatter=1)
+        gx.generate_keys(k, spec)
+        iv = torch.empty(rows, dtype=torch.int64, device="cuda")
+        gx.generate_values(iv, gx.gen_spec(seed=1, stream_id=1, lo=0, hi=1 << 31))
+        fv = torch.empty(rows, dtype=torch.float64, device="cuda")
+        gx.generate_values(fv, gx.gen_spec(seed=1, stream_id=2))
+        kb = 4 if kdt == "int32" else 8
+        for name, algo in (("hash", gx.HASH), ("sort", gx.SORT), ("partition", gx.PARTITION)):
+            def step():
+                return gx.groupby([k], [iv, fv], reqs, gx.make_hint(algo, G))
+            r = step()
+            ng = r.num_rows
+            del r
+            ms = time_steps(torch, step, 2, 1, dist) / 2
+            alg = rows * (kb + 16) + ng * (kb + 56)
+            out.append({"key": kdt, "zipf": z, "groups": G, "algo": name, "ms": round(ms, 3),
+                        "grows_s": round(rows / ms / 1e6, 2),
+                        "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)})
+        del k, iv, fv, cdf
+        torch.cuda.empty_cache()
+    return out
 
 
 def run_sweep(args) -> None:
@@ -585,6 +630,7 @@ def main() -> None:
     ap.add_argument("--batch-instances", type=int, default=512, help="batched pipeline instances (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true", help="skip the oracle check of the timed step's output")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the group-by sweep grid in the bench line")
     ap.add_argument("--cpu-rows", type=int, default=1 << 24)
     ap.add_argument("--traffic", type=float, default=None,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
