@@ -13,9 +13,9 @@
 // A row finds or inserts its string in its instance's table — one 64-bit
 // word per slot holding a 24-bit hash tag and the representative row, so a
 // single CAS publishes a new entry and the bytes are compared against the
-// representative row of the input — gets the next dictionary code on
-// insert, and adds its amount / count to the slot when it passes the date
-// filter.  A finalize kernel writes the per-code results.  Both kernels and
+// representative row of the input, both read as 8-byte chunks of aligned
+// words — gets the next dictionary code on insert, and adds its amount /
+// count to the slot when it passes the date filter.  A finalize kernel writes the per-code results.  Both kernels and
 // the resets are captured once into a CUDA graph and replayed.  Tile size and
 // table load factor are chosen by timing the candidates on the batch.
 //
@@ -47,6 +47,7 @@ struct inst_dev {
     int32_t lo, hi;
     int64_t table_off;   // slot offset of this instance's table
     int64_t result_off;  // code offset of this instance's results
+    int64_t clo, chi;    // byte range of chars the strings occupy: offsets[0], offsets[rows]
 };
 
 struct work_item {
@@ -75,19 +76,52 @@ struct batch_dev {
     long long* out_groups;        // per instance
 };
 
-__device__ __forceinline__ uint64_t fnv1a(const char* p, int64_t len) {
-    uint64_t h = 0xcbf29ce484222325ull;
-    for (int64_t i = 0; i < len; ++i) {
-        h ^= (uint8_t)p[i];
-        h *= 0x100000001b3ull;
-    }
-    return h;
+// String bytes are read in 8-byte chunks assembled from aligned 8-byte words,
+// so the consecutive strings of a warp's lanes come in coalesced words rather
+// than one byte per load.  Every read stays inside the byte range
+// [lo, hi) of `chars` that the column's strings occupy: an aligned word that
+// reaches outside it is assembled from its in-range bytes.
+struct char_span {
+    const unsigned char* chars;
+    int64_t lo, hi;
+};
+
+__device__ __forceinline__ uint64_t word_at(const char_span& c, int64_t a) {
+    // a: position (relative to chars) of an 8-byte-aligned address
+    if (a >= c.lo && a + 8 <= c.hi) return __ldg(reinterpret_cast<const unsigned long long*>(c.chars + a));
+    uint64_t w = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        if (a + k >= c.lo && a + k < c.hi) w |= (uint64_t)c.chars[a + k] << (8 * k);
+    return w;
 }
 
-__device__ __forceinline__ bool str_eq(const char* a, int64_t la, const char* b, int64_t lb) {
+// Bytes [pos, pos + n) of the span, little-endian, n in 1..8, zero above.
+__device__ __forceinline__ uint64_t chunk_at(const char_span& c, int64_t pos, int n) {
+    const int mis = (int)(reinterpret_cast<uintptr_t>(c.chars + pos) & 7);
+    const int64_t a = pos - mis;
+    uint64_t v = word_at(c, a) >> (8 * mis);
+    if (mis + n > 8) v |= word_at(c, a + 8) << (64 - 8 * mis);
+    return n == 8 ? v : (v & ((1ull << (8 * n)) - 1));
+}
+
+// 64-bit hash of the string at [pos, pos + len): a multiply-xorshift round
+// per 8-byte chunk, seeded with the length, finished with fmix64.
+__device__ __forceinline__ uint64_t str_hash(const char_span& c, int64_t pos, int64_t len) {
+    uint64_t h = 0x9E3779B97F4A7C15ull ^ ((uint64_t)len * 0xC2B2AE3D27D4EB4Full);
+    for (int64_t i = 0; i < len; i += 8) {
+        h = (h ^ chunk_at(c, pos + i, (int)(len - i < 8 ? len - i : 8))) * 0xff51afd7ed558ccdull;
+        h ^= h >> 32;
+    }
+    return fmix64(h);
+}
+
+__device__ __forceinline__ bool str_eq(const char_span& c, int64_t pa, int64_t la, int64_t pb, int64_t lb) {
     if (la != lb) return false;
-    for (int64_t i = 0; i < la; ++i)
-        if (a[i] != b[i]) return false;
+    for (int64_t i = 0; i < la; i += 8) {
+        const int n = (int)(la - i < 8 ? la - i : 8);
+        if (chunk_at(c, pa + i, n) != chunk_at(c, pb + i, n)) return false;
+    }
     return true;
 }
 
@@ -95,10 +129,10 @@ __device__ __forceinline__ bool str_eq(const char* a, int64_t la, const char* b,
 __device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst_dev& in, int inst_id, int64_t r,
                                                   bool* inserted) {
     *inserted = false;
+    const char_span sp{reinterpret_cast<const unsigned char*>(in.chars), in.clo, in.chi};
     const int64_t o0 = in.offsets[r], o1 = in.offsets[r + 1];
-    const char* s = in.chars + o0;
     const int64_t len = o1 - o0;
-    const uint64_t h = fnv1a(s, len);
+    const uint64_t h = str_hash(sp, o0, len);
     const uint64_t tag = h >> 40;
     const uint64_t mine = (tag << 40) | (uint64_t)(r + 1);
     const uint32_t mask = b.slots - 1;
@@ -116,8 +150,7 @@ __device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst
         }
         if ((e >> 40) == tag) {
             int64_t rr = (int64_t)(e & ROW_MASK) - 1;
-            if (str_eq(in.chars + in.offsets[rr], in.offsets[rr + 1] - in.offsets[rr], s, len))
-                return in.table_off + slot;
+            if (str_eq(sp, in.offsets[rr], in.offsets[rr + 1] - in.offsets[rr], o0, len)) return in.table_off + slot;
         }
         slot = (slot + 1) & mask;
     }
@@ -185,6 +218,7 @@ struct enc_dev {
     int* overflow;
     uint32_t slots;
     int32_t* codes;
+    int64_t clo, chi;  // byte range of chars the strings occupy: offsets[0], offsets[rows]
 };
 
 __device__ __forceinline__ int64_t enc_find(const enc_dev& e, int64_t r, bool insert, bool* inserted) {
@@ -196,11 +230,14 @@ __device__ __forceinline__ int64_t enc_find(const enc_dev& e, int64_t r, bool in
     in.chars = e.chars;
     in.offsets = e.offsets;
     in.table_off = 0;
+    in.clo = e.clo;
+    in.chi = e.chi;
     if (insert) return find_or_insert(b, in, 0, r, inserted);
     // lookup only: the insert pass has published every string
     *inserted = false;
+    const char_span sp{reinterpret_cast<const unsigned char*>(e.chars), e.clo, e.chi};
     const int64_t o0 = e.offsets[r], len = e.offsets[r + 1] - o0;
-    const uint64_t h = fnv1a(e.chars + o0, len), tag = h >> 40;
+    const uint64_t h = str_hash(sp, o0, len), tag = h >> 40;
     const uint32_t mask = e.slots - 1;
     uint32_t slot = (uint32_t)h & mask;
     for (uint32_t p = 0; p <= mask; ++p) {
@@ -208,7 +245,7 @@ __device__ __forceinline__ int64_t enc_find(const enc_dev& e, int64_t r, bool in
         if (en == 0) return -1;
         if ((en >> 40) == tag) {
             int64_t rr = (int64_t)(en & ROW_MASK) - 1;
-            if (str_eq(e.chars + e.offsets[rr], e.offsets[rr + 1] - e.offsets[rr], e.chars + o0, len)) return slot;
+            if (str_eq(sp, e.offsets[rr], e.offsets[rr + 1] - e.offsets[rr], o0, len)) return slot;
         }
         slot = (slot + 1) & mask;
     }
@@ -291,6 +328,7 @@ __global__ void k_first_rows(const unsigned long long* __restrict__ entries, con
 
 struct gx_batch_plan {
     std::vector<gx_batch_instance> inst;
+    std::vector<int64_t> span_lo, span_hi;  // per instance: offsets[0], offsets[rows]
     std::vector<gx::inst_dev> hinst;
     int64_t max_distinct = 0;
     uint32_t slots = 0;
@@ -329,6 +367,8 @@ static void batch_layout(gx_batch_plan* p, int tile, int lf, cudaStream_t s) {
         d.hi = b.date_hi;
         d.table_off = (int64_t)i * p->slots;
         d.result_off = (int64_t)i * p->max_distinct;
+        d.clo = p->span_lo[i];
+        d.chi = p->span_hi[i];
         p->hinst[i] = d;
         for (int64_t r = 0; r < b.rows; r += tile) work.push_back({i, 0, r, std::min<int64_t>(b.rows, r + tile)});
     }
@@ -482,7 +522,8 @@ static void batch_run_plain(gx_batch_plan* p, cudaStream_t s) {
         GX_CUDA(cudaMemsetAsync(ent.get(), 0, (size_t)slots * 8, s));
         GX_CUDA(cudaMemsetAsync(ds.get(), 0, 16, s));
         enc_dev e{b.chars, b.offsets, rows, ent.get<unsigned long long>(), cos.get<unsigned>(), ds.get<unsigned>(),
-                  reinterpret_cast<int*>(ds.get<char>() + 8), slots, codes.get<int32_t>()};
+                  reinterpret_cast<int*>(ds.get<char>() + 8), slots, codes.get<int32_t>(), p->span_lo[i],
+                  p->span_hi[i]};
         if (rows > 0) {
             k_enc_insert<<<grid_for(rows, 256, 4), 256, 0, s>>>(e);
             GX_LAUNCHED();
@@ -557,6 +598,11 @@ void dictionary_encode_strings(const gx_column_view& v, int64_t size_hint, cudaS
         const gx_string_columns* sc = static_cast<const gx_string_columns*>(v.data);
         require(sc->chars && sc->offsets, "dictionary_encode_strings: null chars or offsets");
         int64_t bound = size_hint > 0 ? std::min(size_hint, rows) : std::min<int64_t>(rows, 1 << 22);
+        // Byte range of chars these rows' strings occupy (reads stay inside it).
+        int64_t span[2];
+        GX_CUDA(cudaMemcpyAsync(&span[0], sc->offsets + v.offset, 8, cudaMemcpyDeviceToHost, s));
+        GX_CUDA(cudaMemcpyAsync(&span[1], sc->offsets + v.offset + rows, 8, cudaMemcpyDeviceToHost, s));
+        GX_CUDA(cudaStreamSynchronize(s));
         bool done = false;
         for (int attempt = 0; attempt < 8 && !done; ++attempt) {
             uint32_t slots = (uint32_t)next_pow2((uint64_t)std::max<int64_t>(64, 2 * bound));
@@ -564,7 +610,8 @@ void dictionary_encode_strings(const gx_column_view& v, int64_t size_hint, cudaS
             GX_CUDA(cudaMemsetAsync(ent.get(), 0, (size_t)slots * 8, s));
             GX_CUDA(cudaMemsetAsync(ds.get(), 0, 16, s));
             enc_dev e{sc->chars, sc->offsets + v.offset, rows, ent.get<unsigned long long>(), cos.get<unsigned>(),
-                      ds.get<unsigned>(), reinterpret_cast<int*>(ds.get<char>() + 8), slots, codes.buf.get<int32_t>()};
+                      ds.get<unsigned>(), reinterpret_cast<int*>(ds.get<char>() + 8), slots, codes.buf.get<int32_t>(),
+                      span[0], span[1]};
             k_enc_insert<<<grid_for(rows, 256, 4), 256, 0, s>>>(e);
             GX_LAUNCHED();
             unsigned hds[4];
@@ -621,6 +668,17 @@ gx_status gx_batch_plan_create(const gx_batch_instance* instances, int32_t count
             gx::require(b.rows == 0 || (b.chars && b.offsets && b.date && b.amount), "batch: null column pointer");
             p->inst.push_back(b);
         }
+        // Byte range of chars each instance's strings occupy: offsets[0] and
+        // offsets[rows], read once (string reads stay inside it).
+        p->span_lo.assign(count, 0);
+        p->span_hi.assign(count, 0);
+        for (int i = 0; i < count; ++i)
+            if (instances[i].rows > 0) {
+                GX_CUDA(cudaMemcpyAsync(&p->span_lo[i], instances[i].offsets, 8, cudaMemcpyDeviceToHost, s));
+                GX_CUDA(cudaMemcpyAsync(&p->span_hi[i], instances[i].offsets + instances[i].rows, 8,
+                                        cudaMemcpyDeviceToHost, s));
+            }
+        GX_CUDA(cudaStreamSynchronize(s));
         p->max_distinct = max_distinct;
         gx::batch_autotune(p.get(), s);
         *plan = p.release();

@@ -311,7 +311,12 @@ int selector_choose(const col& key, const agg_plan& plan, int* radix_bits, cudaS
         int bf = 0;
         for (int k = 1; k < GX_SEL_NUM_FANOUTS; ++k)
             if (y[GX_SEL_NUM_VARIANTS + k] < y[GX_SEL_NUM_VARIANTS + bf]) bf = k;
-        *radix_bits = FANOUT_BITS[bf];
+        // The fan-out head overrides the engine's own rule (radix bits from
+        // the group estimate) only for a predicted gain of at least 20% over
+        // one 8-bit pass: a second radix pass costs a full extra scatter, so a
+        // near-tie is not worth the risk of a misprediction.
+        const float gain = y[GX_SEL_NUM_VARIANTS] - y[GX_SEL_NUM_VARIANTS + bf];  // log2 time
+        *radix_bits = (bf == 0 || gain >= 0.263f) ? FANOUT_BITS[bf] : 0;
     }
     return variants[best];
 }
