@@ -15,9 +15,10 @@
 // single CAS publishes a new entry and the bytes are compared against the
 // representative row of the input, both read as 8-byte chunks of aligned
 // words — gets the next dictionary code on insert, and adds its amount /
-// count to the slot when it passes the date filter.  A finalize kernel writes the per-code results.  Both kernels and
-// the resets are captured once into a CUDA graph and replayed.  Tile size and
-// table load factor are chosen by timing the candidates on the batch.
+// count to the slot when it passes the date filter.  A finalize kernel
+// writes the per-code results.  Both kernels and the resets are captured
+// once into a CUDA graph and replayed.  Tile size and table load factor are
+// chosen by timing the candidates on the batch.
 //
 // The plain engine (gx_batch_run_per_instance) runs the same work as one
 // operator sequence per instance: string dictionary encode, filter with
@@ -86,14 +87,38 @@ struct char_span {
     int64_t lo, hi;
 };
 
-__device__ __forceinline__ uint64_t word_at(const char_span& c, int64_t a) {
-    // a: position (relative to chars) of an 8-byte-aligned address
-    if (a >= c.lo && a + 8 <= c.hi) return __ldg(reinterpret_cast<const unsigned long long*>(c.chars + a));
+// An aligned word that reaches outside the span, assembled from its in-range
+// bytes (kept out of line: it is the rare edge of a column).
+__device__ __noinline__ uint64_t word_at_edge(const char_span& c, int64_t a) {
     uint64_t w = 0;
-#pragma unroll
     for (int k = 0; k < 8; ++k)
         if (a + k >= c.lo && a + k < c.hi) w |= (uint64_t)c.chars[a + k] << (8 * k);
     return w;
+}
+
+__device__ __forceinline__ uint64_t word_at(const char_span& c, int64_t a) {
+    // a: position (relative to chars) of an 8-byte-aligned address
+    if (a >= c.lo && a + 8 <= c.hi) return __ldg(reinterpret_cast<const unsigned long long*>(c.chars + a));
+    return word_at_edge(c, a);
+}
+
+// The first min(len, 32) bytes of the string at [pos, pos + len) as four
+// little-endian 8-byte chunks (zero past the string), from at most five
+// aligned words, in straight-line code.
+__device__ __forceinline__ void load32(const char_span& c, int64_t pos, int64_t len, uint64_t (&ch)[4]) {
+    const int mis = (int)(reinterpret_cast<uintptr_t>(c.chars + pos) & 7);
+    const int64_t a = pos - mis;
+    const int n = (int)(len < 32 ? len : 32);
+    const int nw = (mis + n + 7) >> 3;
+    uint64_t w[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) w[j] = j < nw ? word_at(c, a + 8 * j) : 0ull;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const uint64_t v = mis ? ((w[i] >> (8 * mis)) | (w[i + 1] << (64 - 8 * mis))) : w[i];
+        const int rem = n - 8 * i;
+        ch[i] = rem >= 8 ? v : (rem <= 0 ? 0ull : (v & ((1ull << (8 * rem)) - 1)));
+    }
 }
 
 // Bytes [pos, pos + n) of the span, little-endian, n in 1..8, zero above.
@@ -105,24 +130,47 @@ __device__ __forceinline__ uint64_t chunk_at(const char_span& c, int64_t pos, in
     return n == 8 ? v : (v & ((1ull << (8 * n)) - 1));
 }
 
-// 64-bit hash of the string at [pos, pos + len): a multiply-xorshift round
-// per 8-byte chunk, seeded with the length, finished with fmix64.
-__device__ __forceinline__ uint64_t str_hash(const char_span& c, int64_t pos, int64_t len) {
+// One multiply-xorshift round of the string hash over an 8-byte chunk.
+__device__ __forceinline__ uint64_t hash_round(uint64_t h, uint64_t chunk) {
+    h = (h ^ chunk) * 0xff51afd7ed558ccdull;
+    return h ^ (h >> 32);
+}
+
+// Hash of the string whose first 32 bytes are in ch (load32) and whose
+// remaining bytes, if any, follow at pos + 32.
+__device__ __forceinline__ uint64_t str_hash_chunks(const char_span& c, int64_t pos, int64_t len,
+                                                    const uint64_t (&ch)[4]) {
     uint64_t h = 0x9E3779B97F4A7C15ull ^ ((uint64_t)len * 0xC2B2AE3D27D4EB4Full);
-    for (int64_t i = 0; i < len; i += 8) {
-        h = (h ^ chunk_at(c, pos + i, (int)(len - i < 8 ? len - i : 8))) * 0xff51afd7ed558ccdull;
-        h ^= h >> 32;
-    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        if (8 * i < len) h = hash_round(h, ch[i]);
+    for (int64_t i = 32; i < len; i += 8) h = hash_round(h, chunk_at(c, pos + i, (int)(len - i < 8 ? len - i : 8)));
     return fmix64(h);
 }
 
-__device__ __forceinline__ bool str_eq(const char_span& c, int64_t pa, int64_t la, int64_t pb, int64_t lb) {
+// 64-bit hash of the string at [pos, pos + len): a multiply-xorshift round
+// per 8-byte chunk, seeded with the length, finished with fmix64.
+__device__ __forceinline__ uint64_t str_hash(const char_span& c, int64_t pos, int64_t len) {
+    uint64_t ch[4];
+    load32(c, pos, len, ch);
+    return str_hash_chunks(c, pos, len, ch);
+}
+
+// Does the string at [pa, pa + la) equal the one at pb whose first 32 bytes
+// are in chb (load32)?
+__device__ __forceinline__ bool str_eq_chunks(const char_span& c, int64_t pa, int64_t la, int64_t pb, int64_t lb,
+                                              const uint64_t (&chb)[4]) {
     if (la != lb) return false;
-    for (int64_t i = 0; i < la; i += 8) {
+    uint64_t cha[4];
+    load32(c, pa, la, cha);
+    bool eq = true;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) eq &= cha[i] == chb[i];
+    for (int64_t i = 32; eq && i < la; i += 8) {
         const int n = (int)(la - i < 8 ? la - i : 8);
-        if (chunk_at(c, pa + i, n) != chunk_at(c, pb + i, n)) return false;
+        eq = chunk_at(c, pa + i, n) == chunk_at(c, pb + i, n);
     }
-    return true;
+    return eq;
 }
 
 // Find or insert row r's string; returns the slot (or -1 on a full table).
@@ -132,7 +180,9 @@ __device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst
     const char_span sp{reinterpret_cast<const unsigned char*>(in.chars), in.clo, in.chi};
     const int64_t o0 = in.offsets[r], o1 = in.offsets[r + 1];
     const int64_t len = o1 - o0;
-    const uint64_t h = str_hash(sp, o0, len);
+    uint64_t ch[4];
+    load32(sp, o0, len, ch);
+    const uint64_t h = str_hash_chunks(sp, o0, len, ch);
     const uint64_t tag = h >> 40;
     const uint64_t mine = (tag << 40) | (uint64_t)(r + 1);
     const uint32_t mask = b.slots - 1;
@@ -150,7 +200,8 @@ __device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst
         }
         if ((e >> 40) == tag) {
             int64_t rr = (int64_t)(e & ROW_MASK) - 1;
-            if (str_eq(sp, in.offsets[rr], in.offsets[rr + 1] - in.offsets[rr], o0, len)) return in.table_off + slot;
+            if (str_eq_chunks(sp, in.offsets[rr], in.offsets[rr + 1] - in.offsets[rr], o0, len, ch))
+                return in.table_off + slot;
         }
         slot = (slot + 1) & mask;
     }
@@ -237,7 +288,9 @@ __device__ __forceinline__ int64_t enc_find(const enc_dev& e, int64_t r, bool in
     *inserted = false;
     const char_span sp{reinterpret_cast<const unsigned char*>(e.chars), e.clo, e.chi};
     const int64_t o0 = e.offsets[r], len = e.offsets[r + 1] - o0;
-    const uint64_t h = str_hash(sp, o0, len), tag = h >> 40;
+    uint64_t ch[4];
+    load32(sp, o0, len, ch);
+    const uint64_t h = str_hash_chunks(sp, o0, len, ch), tag = h >> 40;
     const uint32_t mask = e.slots - 1;
     uint32_t slot = (uint32_t)h & mask;
     for (uint32_t p = 0; p <= mask; ++p) {
@@ -245,7 +298,7 @@ __device__ __forceinline__ int64_t enc_find(const enc_dev& e, int64_t r, bool in
         if (en == 0) return -1;
         if ((en >> 40) == tag) {
             int64_t rr = (int64_t)(en & ROW_MASK) - 1;
-            if (str_eq(sp, e.offsets[rr], e.offsets[rr + 1] - e.offsets[rr], o0, len)) return slot;
+            if (str_eq_chunks(sp, e.offsets[rr], e.offsets[rr + 1] - e.offsets[rr], o0, len, ch)) return slot;
         }
         slot = (slot + 1) & mask;
     }
