@@ -520,6 +520,225 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// Unit aggregation with dense group ids (4-byte keys, compiled plans).
+//
+// k_hash_units indexes its accumulators by table slot; at the load the
+// tables run at (<= 1/4) most slots are empty, so replicas do not fit and
+// the lanes of a warp update random slots: ~5.5 bank wavefronts for each
+// 8-byte shared atomic, ~3.5 for a 4-byte one.  Here each slot word packs
+// key (high half) and a dense group id (low half) handed out by the CTA in
+// insertion order, and the accumulators are indexed by group id with R
+// replicas innermost (lane l updates replica l % R).  With R = 8 the lanes
+// of one replica class share two bank pairs, ~3 wavefronts per 8-byte
+// update and ~1.7 per 4-byte one; the key probe is one 8-byte load.
+//
+// Insertion claims an empty slot with (key, PENDING), takes the next id
+// and publishes (key, id).  A row that finds its key PENDING re-reads the
+// slot a bounded number of times; when the wait, the ids (gcap) or the
+// probe sequence run out the row goes to the global table and the unit is
+// merged there instead of appended.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long UD_EMPTY = ~0ull;
+constexpr uint32_t UD_PENDING = 0xFFFFFFFEu;
+constexpr uint32_t UD_SPILL = 0xFFFFFFFDu;
+constexpr uint32_t UD_WAIT_LIMIT = 1u << 16;
+
+struct dtable {
+    unsigned long long* slots;  // [S] key << 32 | group id
+    uint32_t* gkey;             // [gcap] key of each group id
+    int* fill;                  // ids handed out
+    uint32_t mask, gcap;
+};
+
+__device__ __forceinline__ uint32_t d_find_or_insert(const dtable& t, uint32_t k, uint32_t h) {
+    uint32_t slot = h & t.mask;
+    for (uint32_t p = 0; p <= t.mask; ++p) {
+        unsigned long long cur = ((volatile unsigned long long*)t.slots)[slot];
+        if (cur == UD_EMPTY) {
+            cur = atomicCAS(&t.slots[slot], UD_EMPTY, ((unsigned long long)k << 32) | UD_PENDING);
+            if (cur == UD_EMPTY) {
+                uint32_t g = (uint32_t)atomicAdd(t.fill, 1);
+                if (g < t.gcap) t.gkey[g] = k;
+                else g = UD_SPILL;
+                ((volatile unsigned long long*)t.slots)[slot] = ((unsigned long long)k << 32) | g;
+                return g;
+            }
+        }
+        if ((uint32_t)(cur >> 32) == k) {
+            uint32_t g = (uint32_t)cur;
+            for (uint32_t w = 0; g == UD_PENDING && w < UD_WAIT_LIMIT; ++w)
+                g = (uint32_t)((volatile unsigned long long*)t.slots)[slot];
+            return g == UD_PENDING ? UD_SPILL : g;
+        }
+        slot = (slot + 1) & t.mask;
+    }
+    return UD_SPILL;
+}
+
+template <int NV, class... ACCS>
+__global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const uint32_t* __restrict__ keys, int key_kind,
+                                                            agg_desc d, const part_unit* __restrict__ units,
+                                                            const int64_t* __restrict__ n_units, uint32_t s_slots,
+                                                            uint32_t gcap, int reps, int shift, gtable g,
+                                                            uint64_t* __restrict__ out_recs,
+                                                            unsigned long long* __restrict__ out_count,
+                                                            int64_t rec_cap, int* __restrict__ rec_ovf) {
+    static_assert(sizeof...(ACCS) > 0, "compiled plans only");
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_fill, s_spill;
+    __shared__ unsigned long long s_base;
+    __shared__ uint32_t s_q[HGB_NT / 32][31 + 32 * HU_UNROLL];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    constexpr int NA = (int)sizeof...(ACCS);
+    const size_t GR = (size_t)gcap * reps;
+    dtable t;
+    t.slots = reinterpret_cast<unsigned long long*>(smem);
+    t.gkey = reinterpret_cast<uint32_t*>(smem + (size_t)s_slots * 8);
+    unsigned* counts = reinterpret_cast<unsigned*>(smem + (size_t)s_slots * 8 + (((size_t)gcap * 4 + 15) & ~size_t(15)));
+    uint64_t* acc = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(counts) + ((GR * 4 + 15) & ~size_t(15)));
+    t.fill = &s_fill;
+    t.mask = s_slots - 1;
+    t.gcap = gcap;
+    const int rep = (int)(threadIdx.x % (unsigned)reps);
+    unsigned* my_counts = counts + rep;
+    uint64_t* my_acc = acc + rep;
+    const int64_t nu = *n_units;
+    for (int64_t u = blockIdx.x; u < nu; u += gridDim.x) {
+        const part_unit un = units[u];
+        for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) t.slots[i] = UD_EMPTY;
+        for (uint32_t i = threadIdx.x; i < GR; i += HGB_NT) counts[i] = 0;
+        for (int a = 0; a < NA; ++a) {
+            const uint64_t idv = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
+            uint64_t* base = acc + (size_t)a * GR;
+            for (uint32_t i = threadIdx.x; i < GR; i += HGB_NT) base[i] = idv;
+        }
+        if (threadIdx.x == 0) { s_fill = 0; s_spill = 0; }
+        __syncthreads();
+        const int64_t tile = (int64_t)HGB_NT * HU_UNROLL;
+        auto drain = [&](uint32_t off, bool live) {
+            const int64_t i = un.begin + off;
+            uint32_t kq = 0;
+            uint64_t vq[NV];
+            if (live) {
+                kq = (uint32_t)canon32(__ldg(keys + i), key_kind);
+#pragma unroll
+                for (int c = 0; c < NV; ++c) vq[c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
+            }
+            const uint32_t hq = live ? key_hash<4>(kq) : 0u;
+            const uint32_t gq = live ? d_find_or_insert(t, kq, hq >> shift) : UD_SPILL;
+            __syncwarp();
+            if (!live) return;
+            if (gq < gcap) {
+                atomicAdd(&my_counts[gq * reps], 1u);
+                spec::apply_all<0, ACCS...>(my_acc, (uint32_t)GR, gq * reps, vq);
+            } else {
+                if (!s_spill) s_spill = 1;
+                uint64_t* r = g_find_or_insert<4>(g, d, kq, hq);
+                if (r) g_update(r, d, vq, 1ull);
+            }
+        };
+        int qfill = 0;
+        for (int64_t base = un.begin; base < un.end; base += tile) {
+            uint32_t kw[HU_UNROLL];
+            uint64_t v[HU_UNROLL][NV];
+#pragma unroll
+            for (int q = 0; q < HU_UNROLL; ++q) {
+                const int64_t i = base + q * HGB_NT + threadIdx.x;
+                if (i < un.end) {
+                    kw[q] = (uint32_t)canon32(__ldg(keys + i), key_kind);
+#pragma unroll
+                    for (int c = 0; c < NV; ++c)
+                        v[q][c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
+                }
+            }
+            // First probe of every row at once; a row whose home slot holds
+            // another key (or a PENDING / spilled id) is queued for drain.
+            uint32_t gid[HU_UNROLL];
+#pragma unroll
+            for (int q = 0; q < HU_UNROLL; ++q) {
+                const bool valid = base + q * HGB_NT + threadIdx.x < un.end;
+                gid[q] = UD_EMPTY & 0xFFFFFFFFu;
+                if (valid) {
+                    const uint32_t s0 = (key_hash<4>(kw[q]) >> shift) & t.mask;
+                    const unsigned long long cur = ((volatile unsigned long long*)t.slots)[s0];
+                    if ((uint32_t)(cur >> 32) == kw[q] && (uint32_t)cur < gcap) gid[q] = (uint32_t)cur;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < HU_UNROLL; ++q) {
+                const int64_t i = base + q * HGB_NT + threadIdx.x;
+                const bool valid = i < un.end;
+                const bool hit = valid && gid[q] < gcap;
+                const bool miss = valid && !hit;
+                const unsigned mm = __ballot_sync(0xffffffffu, miss);
+                if (miss) s_q[warp][qfill + __popc(mm & lt)] = (uint32_t)(i - un.begin);
+                qfill += __popc(mm);
+                if (hit) {
+                    atomicAdd(&my_counts[gid[q] * reps], 1u);
+                    spec::apply_all<0, ACCS...>(my_acc, (uint32_t)GR, gid[q] * reps, v[q]);
+                }
+            }
+            __syncwarp();
+            while (qfill >= 32) {
+                qfill -= 32;
+                drain(s_q[warp][qfill + lane], true);
+            }
+        }
+        drain(lane < qfill ? s_q[warp][lane] : 0u, lane < qfill);
+        qfill = 0;
+        __syncthreads();
+        const uint32_t ng = min((uint32_t)s_fill, gcap);
+        const bool final_groups = !un.split && !s_spill;
+        if (final_groups) {
+            if (threadIdx.x == 0) {
+                s_base = atomicAdd(out_count, (unsigned long long)ng);
+                if ((int64_t)(s_base + ng) > rec_cap) atomicExch(rec_ovf, 1);
+            }
+            __syncthreads();
+        }
+        const bool append = final_groups && (int64_t)(s_base + ng) <= rec_cap;
+        if (append || !final_groups) {
+            // Ids are dense: group j of the unit is record s_base + j.
+            for (uint32_t j = threadIdx.x; j < ng; j += HGB_NT) {
+                const uint64_t kwv = (uint64_t)t.gkey[j];
+                unsigned long long c = 0;
+                int first = -1;
+                for (int rp = 0; rp < reps; ++rp) {
+                    const unsigned cr = counts[(size_t)j * reps + rp];
+                    c += cr;
+                    if (cr && first < 0) first = rp;
+                }
+                uint64_t* r;
+                if (append) {
+                    r = out_recs + (s_base + j) * d.rec_words;
+                    r[0] = kwv;
+                    if (d.has_count) r[d.count_word] = c;
+                } else {
+                    if (first < 0) continue;
+                    r = g_find_or_insert<4>(g, d, kwv, key_hash<4>(kwv));
+                    if (!r) continue;
+                    if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), c);
+                }
+                for (int a = 0; a < NA; ++a) {
+                    uint64_t x = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
+                    if (first >= 0) {
+                        x = acc[(size_t)a * GR + (size_t)j * reps + first];
+                        for (int rp = first + 1; rp < reps; ++rp)
+                            if (counts[(size_t)j * reps + rp])
+                                x = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], x,
+                                                      acc[(size_t)a * GR + (size_t)j * reps + rp]);
+                    }
+                    if (append) r[d.acc_word0 + a] = x;
+                    else dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], x);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // Initialise `nrec` records: key word = empty, count 0, accumulators = identity.
 __global__ void k_init_records(uint64_t* __restrict__ recs, int64_t nrec, int rec_words, uint64_t empty,
                                agg_desc d) {
@@ -660,6 +879,32 @@ static bool try_units_spec(int grid, size_t smem, cudaStream_t s, const agg_desc
     return true;
 }
 
+template <int NV, class... ACCS>
+static bool try_units_dense(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a,
+                            uint32_t gcap) {
+    if (d.n_cols != NV || !plan_matches<ACCS...>(d)) return false;
+    GX_PROF("partition_aggregate", s);
+    GX_CUDA(cudaFuncSetAttribute(k_units_dense<NV, ACCS...>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_units_dense<NV, ACCS...><<<grid, HGB_NT, smem, s>>>(static_cast<const uint32_t*>(a.keys), a.kind, d, a.units,
+                                                          a.n_units, a.slots, gcap, a.reps, a.shift, a.g, a.orec,
+                                                          a.ocount, a.rec_cap, a.rec_ovf);
+    return true;
+}
+// The dense-id kernel for 4-byte keys and a compiled plan; false when the
+// plan has no compiled form.
+static bool units_dense_dispatch(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a,
+                                 uint32_t gcap) {
+    using namespace spec;
+    if (getenv("GX_HASH_GENERIC")) return false;
+    if (try_units_dense<1, A<OP_SUM, VK_I, 0>>(grid, smem, s, d, a, gcap)) return true;
+    if (try_units_dense<1, A<OP_SUM, VK_F, 0>>(grid, smem, s, d, a, gcap)) return true;
+    if (try_units_dense<2, A<OP_SUM, VK_I, 0>, A<OP_MIN, VK_I, 0>, A<OP_MAX, VK_I, 0>, A<OP_SUM, VK_F, 1>,
+                        A<OP_MIN, VK_F, 1>, A<OP_MAX, VK_F, 1>>(grid, smem, s, d, a, gcap))
+        return true;
+    if (try_units_dense<2, A<OP_SUM, VK_I, 0>, A<OP_SUM, VK_I, 1>>(grid, smem, s, d, a, gcap)) return true;
+    return false;
+}
+
 template <int KW>
 static void units_dispatch(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a) {
     using namespace spec;
@@ -774,6 +1019,27 @@ bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d,
     // 1024 × 3 replicas: 3.26 ms).
     const double gmax = (double)gpp + 4.0 * std::sqrt((double)gpp) + 8.0;
     uint32_t slots = (uint32_t)next_pow2((uint64_t)std::max(64.0, 4.0 * gmax));
+    const int grid = dev().sm_count;
+    if (kw == 4 && !getenv("GX_UNITS_SLOT_TABLE")) {
+        // Dense group ids: slot words (8 B) at load <= 1/4, ids for the
+        // fullest partition expected, and as many replicas (a power of two,
+        // at most 16) as the budget holds.
+        const uint32_t ids = (uint32_t)((((uint64_t)std::ceil(gmax)) + 31) & ~uint64_t(31));
+        const size_t fixed = (size_t)slots * 8 + (((size_t)ids * 4 + 15) & ~size_t(15));
+        auto need = [&](size_t r) {
+            return fixed + (((size_t)ids * r * 4 + 15) & ~size_t(15)) + (size_t)ids * r * 8 * d.n_acc;
+        };
+        size_t r = 16;
+        while (r > 1 && need(r) > budget) r >>= 1;
+        if (need(r) <= budget) {
+            const units_args a{keys, kind, units, n_units, slots, (int)r, shift,
+                               gtable{grec, gcap - 1, gflags, gflags + 1}, orec, ocount, rec_cap, rec_ovf};
+            if (units_dense_dispatch(grid, need(r), s, d, a, ids)) {
+                GX_LAUNCHED();
+                return true;
+            }
+        }
+    }
     // When load 1/4 does not fit (e.g. ~512 groups per partition with 7
     // aggregates), load 1/2 still beats the per-partition fallback kernel
     // by 3x (19.5 -> ~6.5 ms at 2^26.8 rows, 2^17 groups).
@@ -786,7 +1052,6 @@ bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d,
                         (size_t)slots * reps * 8 * d.n_acc;
     units_args a{keys, kind, units, n_units, slots, (int)reps, shift,
                  gtable{grec, gcap - 1, gflags, gflags + 1}, orec, ocount, rec_cap, rec_ovf};
-    const int grid = dev().sm_count;
     GX_PROF("partition_aggregate", s);
     if (kw == 4) units_dispatch<4>(grid, smem, s, d, a);
     else units_dispatch<8>(grid, smem, s, d, a);

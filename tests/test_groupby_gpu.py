@@ -172,6 +172,25 @@ def test_partition_radix_bits_and_overflow_spill():
         assert_columns_match(got, exp)
 
 
+@pytest.mark.parametrize("slot_table", [False, True])
+def test_partition_units_spill_when_tables_run_out(monkeypatch, slot_table):
+    # A group bound of 2^10 with 16 partitions sizes the unit tables for ~64
+    # groups per partition; each partition holds ~2048.  The dense-id kernel
+    # runs out of ids (the slot-indexed one closes its table): the remaining
+    # keys go to the global table and the units merge there.
+    if slot_table:
+        monkeypatch.setenv("GX_UNITS_SLOT_TABLE", "1")
+    n = 1 << 18
+    key = O.gen_keys(n, np.int32, groups=1 << 15, scatter=1, seed=23)
+    iv = O.gen_values(n, np.int64, lo=-(1 << 35), hi=1 << 35, seed=24)
+    fv = O.gen_values(n, np.float64, seed=25)
+    reqs = [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
+    got, exp, hint = run_both(key, [iv, fv], reqs, gx.PARTITION, bound=1 << 10, radix_bits=4)
+    assert hint.radix_bits == 4
+    assert len(got[0]) == len(exp[0]) > 30000
+    assert_columns_match(got, exp)
+
+
 def test_closed_form_uniform_2_28_property():
     # Full-size property check (groupby_test.hpp:64-74): 2^26 rows of
     # shuffled i % G keys with all-ones values; every group sums to N/G.
@@ -255,10 +274,64 @@ def test_partition_min_max_monotone_values(order):
     assert_columns_match(got, exp)
 
 
+@pytest.mark.parametrize("slot_table", [False, True])
+@pytest.mark.parametrize("pattern", ["late_extremes", "decreasing"])
+def test_partition_min_max_large_units(monkeypatch, pattern, slot_table):
+    # Units of ~56K rows (2^26 rows, 2^12 groups), through the dense-id unit
+    # kernel and the slot-indexed one (GX_UNITS_SLOT_TABLE).
+    # "late_extremes" plants every group's true MIN and MAX (and float NaN,
+    # infinities, signed zeros, int64 limits) in the last eighth of the rows,
+    # long after each group's first rows; "decreasing" makes every row a new
+    # MIN.
+    if slot_table:
+        monkeypatch.setenv("GX_UNITS_SLOT_TABLE", "1")
+    n, G = 1 << 26, 1 << 12
+    key = O.gen_keys(n, np.int32, groups=G, scatter=1, seed=43)
+    idx = np.arange(n, dtype=np.int64)
+    if pattern == "decreasing":
+        iv = (n - idx) * 7 - (1 << 33)
+        fv = 1.0e6 - idx * 0.25
+    else:
+        rng = np.random.default_rng(44)
+        iv = rng.integers(-(1 << 40), 1 << 40, n, dtype=np.int64)
+        fv = rng.random(n) + 0.5  # positive: float SUMs without cancellation
+        late = idx >= n - n // 8
+        pick = late & (rng.random(n) < 0.002)
+        m = int(pick.sum())
+        iv[pick] = np.where(rng.random(m) < 0.5, -(1 << 50), 1 << 50) + rng.integers(-1000, 1000, m)
+        fv[pick] = np.where(rng.random(m) < 0.5, -50.0, 50.0) * (1.0 + rng.random(m))
+        ends = np.nonzero(late & ~pick)[0]
+        e = rng.choice(ends, 64, replace=False)
+        iv[e[:8]] = np.iinfo(np.int64).min
+        iv[e[8:16]] = np.iinfo(np.int64).max
+        fv[e[16:24]] = -np.inf
+        fv[e[24:32]] = np.inf
+        fv[e[32:40]] = np.nan
+        fv[e[40:52]] = -0.0
+        fv[e[52:64]] = 0.0
+    reqs = [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
+    hint = gx.make_hint(gx.PARTITION, G)
+    got = sort_by_key(gx.groupby([to_dev(key)], [to_dev(iv), to_dev(fv)], reqs, hint).numpy_columns())
+    assert hint.groupby_algo == gx.PARTITION
+    exp = O.groupby(key, [iv, fv], [(c, OKIND[k]) for c, k in reqs])
+    for c in (0, 2, 3, 7):
+        assert np.array_equal(got[c], exp[c]), c
+    for c in (5, 6):
+        assert np.array_equal(got[c], exp[c], equal_nan=True), c
+    if pattern == "late_extremes":
+        # the planted values are the extremes of the groups that got one
+        assert (got[2] <= -(1 << 50) + 1000).sum() > G // 4
+        assert (got[5] <= -50.0).sum() > G // 4
+    # Integer SUM wraps identically; float SUM within tolerance (or NaN / inf
+    # where the group holds one).
+    assert_columns_match(got, exp)
+
+
 @pytest.mark.parametrize("env,algo,G", [
     ("GX_HASH_GENERIC", gx.HASH, 4096),      # run-time aggregation list instead of a compiled plan
     ("GX_HASH_GENERIC", gx.PARTITION, 1 << 16),
     ("GX_PART_OLD_AGG", gx.PARTITION, 1 << 16),  # per-partition CTA aggregation kernel
+    ("GX_UNITS_SLOT_TABLE", gx.PARTITION, 1 << 16),  # slot-indexed unit tables instead of dense group ids
 ])
 def test_forced_alternative_kernels(monkeypatch, env, algo, G):
     # The switches route a plan through its alternative kernel; results must
