@@ -47,22 +47,27 @@ def measured_peaks() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) during the timed region."""
+    """nvidia-smi samples every 25 ms around the timed region: `ready()`
+    waits (bounded) for the first sample so a slow nvidia-smi start cannot
+    miss a short region, `window()` marks the region, and the summary keeps
+    the samples taken inside it (one interval of slack on each side)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 25
 
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.INTERVAL_MS)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -71,7 +76,15 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def ready(self, timeout_s: float = 10.0) -> None:
+        end = time.monotonic() + timeout_s
+        while self.proc and not self.lines and time.monotonic() < end and self.proc.poll() is None:
+            time.sleep(0.01)
+
+    def window(self, t0: float, t1: float) -> None:
+        self.t0, self.t1 = t0, t1
 
     def __exit__(self, *exc):
         if self.proc:
@@ -84,7 +97,10 @@ class ClockSampler:
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        slack = self.INTERVAL_MS / 1000.0
+        picked = [ln for t, ln in self.lines
+                  if self.t0 is None or self.t0 - slack <= t <= self.t1 + slack]
+        for ln in picked:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -120,13 +136,17 @@ def groupby_reqs(gx):
     return [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
 
 
-def time_steps(torch, fn, steps: int, warmup: int, dist=None) -> float:
-    """Device time (ms) of `steps` calls, CUDA events on the current stream."""
+def time_steps(torch, fn, steps: int, warmup: int, dist=None, marks: list | None = None) -> float:
+    """Device time (ms) of `steps` calls, CUDA events on the current stream;
+    `marks` (if given) receives the host clock at the start and end of the
+    timed steps."""
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
+    if marks is not None:
+        marks.append(time.monotonic())
     s = torch.cuda.current_stream()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(s)
@@ -134,6 +154,8 @@ def time_steps(torch, fn, steps: int, warmup: int, dist=None) -> float:
         fn()
     b.record(s)
     torch.cuda.synchronize()
+    if marks is not None:
+        marks.append(time.monotonic())
     ms = a.elapsed_time(b)
     if dist is not None:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -199,7 +221,10 @@ def run_gx(args) -> None:
     gx.lib.gx_profile_reset()
     gx.lib.gx_profile_enable(1)
     with ClockSampler(local) as clk:
-        ms = time_steps(torch, step, args.steps, args.warmup, dist)
+        clk.ready()
+        marks: list = []
+        ms = time_steps(torch, step, args.steps, args.warmup, dist, marks)
+        clk.window(marks[0], marks[1])
     gx.lib.gx_profile_enable(0)
     launches = gx.kernel_launches() - launches0
     in_bytes = rows * (4 + 8 + 8)
@@ -223,11 +248,13 @@ def run_gx(args) -> None:
     # DRAM bytes per row of the partition plan's two kernels on this workload,
     # from one ncu capture at 2^25 rows (dram__bytes_read.sum + dram__bytes_write.sum
     # per launch ÷ 2^25; DRAM bytes grow in proportion to rows), scaled to this run:
-    #   ncu --set full --clock-control none -k regex:"k_hash_units|k_part_scatter_bulk" -s 2 -c 2 \
-    #       python bench.py --rows 33554432 --steps 3 --warmup 3 --no-join --batch-instances 0 --no-cpu
-    # k_hash_units 678.12 + 8.59 MB, k_part_scatter_bulk 688.36 + 621.05 MB (the scatter's
+    #   ncu --set full --clock-control none -k regex:k_units_dense -s 2 -c 1 python bench.py \
+    #       --rows 33554432 --steps 2 --warmup 3 --no-join --batch-instances 0 --no-cpu --no-check --no-sweep
+    #   ncu --set full --clock-control none -k regex:k_part_scatter_bulk -s 2 -c 1 python bench.py \
+    #       --rows 33554432 --steps 3 --warmup 3 --no-join --batch-instances 0 --no-cpu
+    # k_units_dense 677.53 + 7.17 MB, k_part_scatter_bulk 688.36 + 621.05 MB (the scatter's
     # last writes leave L2 after the kernel ends).
-    dram_per_row = {"partition_aggregate": (678.12e6 + 8.59e6) / 2**25,
+    dram_per_row = {"partition_aggregate": (677.53e6 + 7.17e6) / 2**25,
                     "partition_scatter": (688.36e6 + 621.05e6) / 2**25}
     traffic = args.traffic
     if traffic is None and main_kernel in dram_per_row and G == 1 << 16 and algo_name.startswith("partition"):

@@ -187,7 +187,10 @@ void selector_features(const col& key_in, float* f, cudaStream_t s) {
     sc.data = samp.get();
     sc.n = m;
     sc.type = GX_UINT64;
-    radix_sort(sc, nullptr, 0, false, 0, -1, false, sorted.get(), nullptr, nullptr, 0, s);
+    // Keys of 4 bytes or less are sampled zero-extended: their low 32 bits
+    // order them (four 8-bit passes instead of eight).
+    radix_sort(sc, nullptr, 0, false, 0, size_of(key.type) == 8 ? -1 : 32, false, sorted.get(), nullptr, nullptr, 0,
+               s);
     hll_registers(key, m, stride, regs.get<unsigned>(), s);
     std::vector<uint64_t> h(m);
     std::vector<unsigned> hr(8192);
