@@ -521,70 +521,125 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// Unit aggregation with dense group ids (4-byte keys, compiled plans).
+// Unit aggregation with dense group ids (compiled plans).
 //
-// k_hash_units indexes its accumulators by table slot; at the load the
-// tables run at (<= 1/4) most slots are empty, so replicas do not fit and
-// the lanes of a warp update random slots: ~5.5 bank wavefronts for each
-// 8-byte shared atomic, ~3.5 for a 4-byte one.  Here each slot word packs
-// key (high half) and a dense group id (low half) handed out by the CTA in
-// insertion order, and the accumulators are indexed by group id with R
-// replicas innermost (lane l updates replica l % R).  With R = 8 the lanes
-// of one replica class share two bank pairs, ~3 wavefronts per 8-byte
-// update and ~1.7 per 4-byte one; the key probe is one 8-byte load.
+// k_hash_units indexes its accumulators by table slot, and at the load its
+// tables run at (<= 1/4) the slots leave room for one accumulator replica.
+// Here the CTA hands out dense group ids in insertion order and indexes the
+// accumulators by id, R replicas innermost (lane l updates replica l % R):
+// sized by groups instead of slots, 8 replicas fit at ~256 groups per
+// partition with 7 aggregates (2.92 -> 2.60 ms at 2^28 rows, G = 2^16).
 //
-// Insertion claims an empty slot with (key, PENDING), takes the next id
-// and publishes (key, id).  A row that finds its key PENDING re-reads the
-// slot a bounded number of times; when the wait, the ids (gcap) or the
-// probe sequence run out the row goes to the global table and the unit is
-// merged there instead of appended.
+// Slot words: 4-byte keys pack key << 32 | id, so the probe is one load and
+// one compare.  8-byte keys pack id << 32 | 32-bit key hash and keep the key
+// itself in gkey[id]; a row whose hash matches confirms the key there, and a
+// different key with the same hash simply continues the probe walk.
+//
+// Insertion claims an empty slot (id PENDING), takes the next id, writes
+// the key of the id and publishes the slot word.  A row that finds its slot
+// PENDING (or, for 8-byte keys, the id's key not yet visible) re-reads a
+// bounded number of times; when the wait, the ids (gcap) or the probe walk
+// run out, the row goes to the global table and the unit is merged there
+// instead of appended.
 // ---------------------------------------------------------------------------
 constexpr unsigned long long UD_EMPTY = ~0ull;
 constexpr uint32_t UD_PENDING = 0xFFFFFFFEu;
 constexpr uint32_t UD_SPILL = 0xFFFFFFFDu;
 constexpr uint32_t UD_WAIT_LIMIT = 1u << 16;
 
+// Slot word accesses (single 8-byte loads and stores).  For 8-byte keys
+// gkey[] holds UD_UNSET from the start of each unit until an id's key is
+// written (each id is written once per unit), so a read of gkey[id] yields
+// either UD_UNSET or the id's true key: a reader that matches its key there
+// has found its group whatever order the two writes became visible in, and
+// one that reads UD_UNSET waits for the key (bounded).  Keys equal to
+// UD_UNSET go to the global table.  No fence or acquire load is needed on
+// the row path (acquire loads there cost 2.6x at 2^24 groups: they also
+// order the row's earlier value loads).
+constexpr unsigned long long UD_UNSET = 0x8000000000000000ull;
+template <int KW>
+__device__ __forceinline__ unsigned long long ld_slot(const unsigned long long* p) {
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+template <int KW>
+__device__ __forceinline__ void st_slot(unsigned long long* p, unsigned long long v) {
+    *reinterpret_cast<volatile unsigned long long*>(p) = v;
+}
+
+template <int KW>
 struct dtable {
-    unsigned long long* slots;  // [S] key << 32 | group id
-    uint32_t* gkey;             // [gcap] key of each group id
+    using kt = typename std::conditional<KW == 4, uint32_t, unsigned long long>::type;
+    unsigned long long* slots;  // [S] slot words (see above)
+    kt* gkey;                   // [gcap] key of each group id
     int* fill;                  // ids handed out
     uint32_t mask, gcap;
 };
 
-__device__ __forceinline__ uint32_t d_find_or_insert(const dtable& t, uint32_t k, uint32_t h) {
+// Slot word layout per key width: the id and the tag to compare.
+template <int KW>
+__device__ __forceinline__ uint32_t ud_id(unsigned long long w) {
+    return KW == 4 ? (uint32_t)w : (uint32_t)(w >> 32);
+}
+template <int KW>
+__device__ __forceinline__ uint32_t ud_tag(unsigned long long w) {
+    return KW == 4 ? (uint32_t)(w >> 32) : (uint32_t)w;
+}
+template <int KW>
+__device__ __forceinline__ unsigned long long ud_word(uint32_t tag, uint32_t id) {
+    return KW == 4 ? ((unsigned long long)tag << 32) | id : ((unsigned long long)id << 32) | tag;
+}
+
+// Group id of key k (canonical; tag = the key itself for 4-byte keys, its
+// 32-bit hash for 8-byte ones), inserting it; UD_SPILL when the wait, the
+// ids or the probe walk run out.
+template <int KW>
+__device__ __forceinline__ uint32_t d_find_or_insert(const dtable<KW>& t, uint64_t k, uint32_t tag, uint32_t h) {
+    if (KW == 8 && k == UD_UNSET) return UD_SPILL;
     uint32_t slot = h & t.mask;
     for (uint32_t p = 0; p <= t.mask; ++p) {
-        unsigned long long cur = ((volatile unsigned long long*)t.slots)[slot];
+        unsigned long long cur = ld_slot<KW>(&t.slots[slot]);
         if (cur == UD_EMPTY) {
-            cur = atomicCAS(&t.slots[slot], UD_EMPTY, ((unsigned long long)k << 32) | UD_PENDING);
+            cur = atomicCAS(&t.slots[slot], UD_EMPTY, ud_word<KW>(tag, UD_PENDING));
             if (cur == UD_EMPTY) {
                 uint32_t g = (uint32_t)atomicAdd(t.fill, 1);
-                if (g < t.gcap) t.gkey[g] = k;
+                if (g < t.gcap) t.gkey[g] = (typename dtable<KW>::kt)k;
                 else g = UD_SPILL;
-                ((volatile unsigned long long*)t.slots)[slot] = ((unsigned long long)k << 32) | g;
+                st_slot<KW>(&t.slots[slot], ud_word<KW>(tag, g));
                 return g;
             }
         }
-        if ((uint32_t)(cur >> 32) == k) {
-            uint32_t g = (uint32_t)cur;
-            for (uint32_t w = 0; g == UD_PENDING && w < UD_WAIT_LIMIT; ++w)
-                g = (uint32_t)((volatile unsigned long long*)t.slots)[slot];
-            return g == UD_PENDING ? UD_SPILL : g;
+        if (ud_tag<KW>(cur) == tag) {
+            uint32_t g = ud_id<KW>(cur);
+            for (uint32_t w = 0; g == UD_PENDING && w < UD_WAIT_LIMIT; ++w) g = ud_id<KW>(ld_slot<KW>(&t.slots[slot]));
+            if (g == UD_PENDING || g == UD_SPILL) return UD_SPILL;
+            if (KW == 4) return g;
+            const volatile unsigned long long* gk = reinterpret_cast<volatile unsigned long long*>(t.gkey) + g;
+            unsigned long long kk = *gk;
+            for (uint32_t w = 0; kk == UD_UNSET && w < UD_WAIT_LIMIT; ++w) kk = *gk;
+            if (kk == UD_UNSET) return UD_SPILL;
+            if (kk == k) return g;
         }
         slot = (slot + 1) & t.mask;
     }
     return UD_SPILL;
 }
 
-template <int NV, class... ACCS>
-__global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const uint32_t* __restrict__ keys, int key_kind,
-                                                            agg_desc d, const part_unit* __restrict__ units,
+template <int KW>
+__device__ __forceinline__ uint64_t ud_load_key(const void* keys, int64_t i, int kind) {
+    if (KW == 4) return canon32(__ldg(static_cast<const unsigned*>(keys) + i), kind);
+    return canon64(__ldg(static_cast<const unsigned long long*>(keys) + i), kind);
+}
+
+template <int KW, int NV, class... ACCS>
+__global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const void* __restrict__ keys, int key_kind, agg_desc d,
+                                                            const part_unit* __restrict__ units,
                                                             const int64_t* __restrict__ n_units, uint32_t s_slots,
-                                                            uint32_t gcap, int reps, int shift, gtable g,
-                                                            uint64_t* __restrict__ out_recs,
+                                                            uint32_t gcap, int reps, uint32_t gpp, int shift,
+                                                            gtable g, uint64_t* __restrict__ out_recs,
                                                             unsigned long long* __restrict__ out_count,
                                                             int64_t rec_cap, int* __restrict__ rec_ovf) {
     static_assert(sizeof...(ACCS) > 0, "compiled plans only");
+    using kt = typename dtable<KW>::kt;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_fill, s_spill;
     __shared__ unsigned long long s_base;
@@ -592,62 +647,78 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const uint32_t* __res
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     constexpr int NA = (int)sizeof...(ACCS);
-    const size_t GR = (size_t)gcap * reps;
-    dtable t;
+    const size_t GR = (size_t)gcap * reps;  // words per accumulator (layout for `reps` replicas)
+    dtable<KW> t;
     t.slots = reinterpret_cast<unsigned long long*>(smem);
-    t.gkey = reinterpret_cast<uint32_t*>(smem + (size_t)s_slots * 8);
-    unsigned* counts = reinterpret_cast<unsigned*>(smem + (size_t)s_slots * 8 + (((size_t)gcap * 4 + 15) & ~size_t(15)));
+    t.gkey = reinterpret_cast<kt*>(smem + (size_t)s_slots * 8);
+    unsigned* counts =
+        reinterpret_cast<unsigned*>(smem + (size_t)s_slots * 8 + (((size_t)gcap * KW + 15) & ~size_t(15)));
     uint64_t* acc = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(counts) + ((GR * 4 + 15) & ~size_t(15)));
     t.fill = &s_fill;
     t.mask = s_slots - 1;
     t.gcap = gcap;
-    const int rep = (int)(threadIdx.x % (unsigned)reps);
-    unsigned* my_counts = counts + rep;
-    uint64_t* my_acc = acc + rep;
+    // tag of a key in its slot word: the key (4 bytes) or its hash (8 bytes)
+    auto tag_of = [](uint64_t k, uint32_t h) { return KW == 4 ? (uint32_t)k : h; };
     const int64_t nu = *n_units;
     for (int64_t u = blockIdx.x; u < nu; u += gridDim.x) {
         const part_unit un = units[u];
+        // Replicas of this unit: every one for a piece of a split (large)
+        // partition, where a few groups take most rows; otherwise one per 16
+        // rows of a group, since each replica also costs set-up and merge
+        // work (e.g. a 4K-row unit of ~256 groups keeps one).
+        int R = reps;
+        if (!un.split) {
+            const int64_t q = (un.end - un.begin) / (16 * (int64_t)gpp);
+            R = 1;
+            while (R < reps && 2 * (int64_t)R <= q) R *= 2;
+        }
+        const uint32_t GRu = gcap * (uint32_t)R;  // words in use per accumulator
+        const int rep = (int)(threadIdx.x & (unsigned)(R - 1));
+        unsigned* my_counts = counts + rep;
+        uint64_t* my_acc = acc + rep;
         for (uint32_t i = threadIdx.x; i < s_slots; i += HGB_NT) t.slots[i] = UD_EMPTY;
-        for (uint32_t i = threadIdx.x; i < GR; i += HGB_NT) counts[i] = 0;
+        if (KW == 8)
+            for (uint32_t i = threadIdx.x; i < gcap; i += HGB_NT) t.gkey[i] = (kt)UD_UNSET;
+        for (uint32_t i = threadIdx.x; i < GRu; i += HGB_NT) counts[i] = 0;
         for (int a = 0; a < NA; ++a) {
             const uint64_t idv = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
             uint64_t* base = acc + (size_t)a * GR;
-            for (uint32_t i = threadIdx.x; i < GR; i += HGB_NT) base[i] = idv;
+            for (uint32_t i = threadIdx.x; i < GRu; i += HGB_NT) base[i] = idv;
         }
         if (threadIdx.x == 0) { s_fill = 0; s_spill = 0; }
         __syncthreads();
         const int64_t tile = (int64_t)HGB_NT * HU_UNROLL;
         auto drain = [&](uint32_t off, bool live) {
             const int64_t i = un.begin + off;
-            uint32_t kq = 0;
+            kt kq = 0;
             uint64_t vq[NV];
             if (live) {
-                kq = (uint32_t)canon32(__ldg(keys + i), key_kind);
+                kq = (kt)ud_load_key<KW>(keys, i, key_kind);
 #pragma unroll
                 for (int c = 0; c < NV; ++c) vq[c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
             }
-            const uint32_t hq = live ? key_hash<4>(kq) : 0u;
-            const uint32_t gq = live ? d_find_or_insert(t, kq, hq >> shift) : UD_SPILL;
+            const uint32_t hq = live ? key_hash<KW>(kq) : 0u;
+            const uint32_t gq = live ? d_find_or_insert<KW>(t, kq, tag_of(kq, hq), hq >> shift) : UD_SPILL;
             __syncwarp();
             if (!live) return;
             if (gq < gcap) {
-                atomicAdd(&my_counts[gq * reps], 1u);
-                spec::apply_all<0, ACCS...>(my_acc, (uint32_t)GR, gq * reps, vq);
+                atomicAdd(&my_counts[gq * R], 1u);
+                spec::apply_all<0, ACCS...>(my_acc, (uint32_t)GR, gq * R, vq);
             } else {
                 if (!s_spill) s_spill = 1;
-                uint64_t* r = g_find_or_insert<4>(g, d, kq, hq);
+                uint64_t* r = g_find_or_insert<KW>(g, d, kq, hq);
                 if (r) g_update(r, d, vq, 1ull);
             }
         };
         int qfill = 0;
         for (int64_t base = un.begin; base < un.end; base += tile) {
-            uint32_t kw[HU_UNROLL];
+            kt kw[HU_UNROLL];
             uint64_t v[HU_UNROLL][NV];
 #pragma unroll
             for (int q = 0; q < HU_UNROLL; ++q) {
                 const int64_t i = base + q * HGB_NT + threadIdx.x;
                 if (i < un.end) {
-                    kw[q] = (uint32_t)canon32(__ldg(keys + i), key_kind);
+                    kw[q] = (kt)ud_load_key<KW>(keys, i, key_kind);
 #pragma unroll
                     for (int c = 0; c < NV; ++c)
                         v[q][c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
@@ -659,11 +730,15 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const uint32_t* __res
 #pragma unroll
             for (int q = 0; q < HU_UNROLL; ++q) {
                 const bool valid = base + q * HGB_NT + threadIdx.x < un.end;
-                gid[q] = UD_EMPTY & 0xFFFFFFFFu;
+                gid[q] = 0xFFFFFFFFu;
                 if (valid) {
-                    const uint32_t s0 = (key_hash<4>(kw[q]) >> shift) & t.mask;
-                    const unsigned long long cur = ((volatile unsigned long long*)t.slots)[s0];
-                    if ((uint32_t)(cur >> 32) == kw[q] && (uint32_t)cur < gcap) gid[q] = (uint32_t)cur;
+                    const uint32_t h = key_hash<KW>(kw[q]);
+                    const unsigned long long cur = ld_slot<KW>(&t.slots[(h >> shift) & t.mask]);
+                    const uint32_t id = ud_id<KW>(cur);
+                    if (ud_tag<KW>(cur) == tag_of(kw[q], h) && id < gcap &&
+                        (KW == 4 || ((uint64_t)kw[q] != UD_UNSET &&
+                                     (uint64_t)((volatile kt*)t.gkey)[id] == (uint64_t)kw[q])))
+                        gid[q] = id;
                 }
             }
 #pragma unroll
@@ -676,8 +751,8 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const uint32_t* __res
                 if (miss) s_q[warp][qfill + __popc(mm & lt)] = (uint32_t)(i - un.begin);
                 qfill += __popc(mm);
                 if (hit) {
-                    atomicAdd(&my_counts[gid[q] * reps], 1u);
-                    spec::apply_all<0, ACCS...>(my_acc, (uint32_t)GR, gid[q] * reps, v[q]);
+                    atomicAdd(&my_counts[gid[q] * R], 1u);
+                    spec::apply_all<0, ACCS...>(my_acc, (uint32_t)GR, gid[q] * R, v[q]);
                 }
             }
             __syncwarp();
@@ -705,8 +780,8 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const uint32_t* __res
                 const uint64_t kwv = (uint64_t)t.gkey[j];
                 unsigned long long c = 0;
                 int first = -1;
-                for (int rp = 0; rp < reps; ++rp) {
-                    const unsigned cr = counts[(size_t)j * reps + rp];
+                for (int rp = 0; rp < R; ++rp) {
+                    const unsigned cr = counts[(size_t)j * R + rp];
                     c += cr;
                     if (cr && first < 0) first = rp;
                 }
@@ -717,18 +792,18 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const uint32_t* __res
                     if (d.has_count) r[d.count_word] = c;
                 } else {
                     if (first < 0) continue;
-                    r = g_find_or_insert<4>(g, d, kwv, key_hash<4>(kwv));
+                    r = g_find_or_insert<KW>(g, d, kwv, key_hash<KW>(kwv));
                     if (!r) continue;
                     if (d.has_count) atomicAdd((unsigned long long*)(r + d.count_word), c);
                 }
                 for (int a = 0; a < NA; ++a) {
                     uint64_t x = dev_::acc_ident(d.acc_op[a], d.acc_kind[a]);
                     if (first >= 0) {
-                        x = acc[(size_t)a * GR + (size_t)j * reps + first];
-                        for (int rp = first + 1; rp < reps; ++rp)
-                            if (counts[(size_t)j * reps + rp])
+                        x = acc[(size_t)a * GR + (size_t)j * R + first];
+                        for (int rp = first + 1; rp < R; ++rp)
+                            if (counts[(size_t)j * R + rp])
                                 x = dev_::acc_combine(d.acc_op[a], d.acc_kind[a], x,
-                                                      acc[(size_t)a * GR + (size_t)j * reps + rp]);
+                                                      acc[(size_t)a * GR + (size_t)j * R + rp]);
                     }
                     if (append) r[d.acc_word0 + a] = x;
                     else dev_::acc_atomic(r + d.acc_word0 + a, d.acc_op[a], d.acc_kind[a], x);
@@ -879,29 +954,31 @@ static bool try_units_spec(int grid, size_t smem, cudaStream_t s, const agg_desc
     return true;
 }
 
-template <int NV, class... ACCS>
+template <int KW, int NV, class... ACCS>
 static bool try_units_dense(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a,
-                            uint32_t gcap) {
+                            uint32_t gcap, uint32_t gpp) {
     if (d.n_cols != NV || !plan_matches<ACCS...>(d)) return false;
     GX_PROF("partition_aggregate", s);
-    GX_CUDA(cudaFuncSetAttribute(k_units_dense<NV, ACCS...>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_units_dense<NV, ACCS...><<<grid, HGB_NT, smem, s>>>(static_cast<const uint32_t*>(a.keys), a.kind, d, a.units,
-                                                          a.n_units, a.slots, gcap, a.reps, a.shift, a.g, a.orec,
-                                                          a.ocount, a.rec_cap, a.rec_ovf);
+    GX_CUDA(cudaFuncSetAttribute(k_units_dense<KW, NV, ACCS...>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    k_units_dense<KW, NV, ACCS...><<<grid, HGB_NT, smem, s>>>(a.keys, a.kind, d, a.units, a.n_units, a.slots, gcap,
+                                                              a.reps, gpp, a.shift, a.g, a.orec, a.ocount,
+                                                              a.rec_cap, a.rec_ovf);
     return true;
 }
-// The dense-id kernel for 4-byte keys and a compiled plan; false when the
-// plan has no compiled form.
+// The dense-id kernel for a compiled plan; false when the plan has no
+// compiled form.
+template <int KW>
 static bool units_dense_dispatch(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a,
-                                 uint32_t gcap) {
+                                 uint32_t gcap, uint32_t gpp) {
     using namespace spec;
     if (getenv("GX_HASH_GENERIC")) return false;
-    if (try_units_dense<1, A<OP_SUM, VK_I, 0>>(grid, smem, s, d, a, gcap)) return true;
-    if (try_units_dense<1, A<OP_SUM, VK_F, 0>>(grid, smem, s, d, a, gcap)) return true;
-    if (try_units_dense<2, A<OP_SUM, VK_I, 0>, A<OP_MIN, VK_I, 0>, A<OP_MAX, VK_I, 0>, A<OP_SUM, VK_F, 1>,
-                        A<OP_MIN, VK_F, 1>, A<OP_MAX, VK_F, 1>>(grid, smem, s, d, a, gcap))
+    if (try_units_dense<KW, 1, A<OP_SUM, VK_I, 0>>(grid, smem, s, d, a, gcap, gpp)) return true;
+    if (try_units_dense<KW, 1, A<OP_SUM, VK_F, 0>>(grid, smem, s, d, a, gcap, gpp)) return true;
+    if (try_units_dense<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_MIN, VK_I, 0>, A<OP_MAX, VK_I, 0>, A<OP_SUM, VK_F, 1>,
+                        A<OP_MIN, VK_F, 1>, A<OP_MAX, VK_F, 1>>(grid, smem, s, d, a, gcap, gpp))
         return true;
-    if (try_units_dense<2, A<OP_SUM, VK_I, 0>, A<OP_SUM, VK_I, 1>>(grid, smem, s, d, a, gcap)) return true;
+    if (try_units_dense<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_SUM, VK_I, 1>>(grid, smem, s, d, a, gcap, gpp)) return true;
     return false;
 }
 
@@ -1020,12 +1097,12 @@ bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d,
     const double gmax = (double)gpp + 4.0 * std::sqrt((double)gpp) + 8.0;
     uint32_t slots = (uint32_t)next_pow2((uint64_t)std::max(64.0, 4.0 * gmax));
     const int grid = dev().sm_count;
-    if (kw == 4 && !getenv("GX_UNITS_SLOT_TABLE")) {
-        // Dense group ids: slot words (8 B) at load <= 1/4, ids for the
-        // fullest partition expected, and as many replicas (a power of two,
-        // at most 16) as the budget holds.
+    if (!getenv("GX_UNITS_SLOT_TABLE")) {
+        // Dense group ids: slot words (8 B) at load <= 1/4, ids (and their
+        // keys) for the fullest partition expected, and as many replicas (a
+        // power of two, at most 16) as the budget holds.
         const uint32_t ids = (uint32_t)((((uint64_t)std::ceil(gmax)) + 31) & ~uint64_t(31));
-        const size_t fixed = (size_t)slots * 8 + (((size_t)ids * 4 + 15) & ~size_t(15));
+        const size_t fixed = (size_t)slots * 8 + (((size_t)ids * kw + 15) & ~size_t(15));
         auto need = [&](size_t r) {
             return fixed + (((size_t)ids * r * 4 + 15) & ~size_t(15)) + (size_t)ids * r * 8 * d.n_acc;
         };
@@ -1034,7 +1111,9 @@ bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d,
         if (need(r) <= budget) {
             const units_args a{keys, kind, units, n_units, slots, (int)r, shift,
                                gtable{grec, gcap - 1, gflags, gflags + 1}, orec, ocount, rec_cap, rec_ovf};
-            if (units_dense_dispatch(grid, need(r), s, d, a, ids)) {
+            const uint32_t g32 = (uint32_t)std::min<int64_t>(std::max<int64_t>(gpp, 1), ids);
+            if (kw == 4 ? units_dense_dispatch<4>(grid, need(r), s, d, a, ids, g32)
+                        : units_dense_dispatch<8>(grid, need(r), s, d, a, ids, g32)) {
                 GX_LAUNCHED();
                 return true;
             }

@@ -172,8 +172,9 @@ def test_partition_radix_bits_and_overflow_spill():
         assert_columns_match(got, exp)
 
 
+@pytest.mark.parametrize("kdt", [np.int32, np.int64])
 @pytest.mark.parametrize("slot_table", [False, True])
-def test_partition_units_spill_when_tables_run_out(monkeypatch, slot_table):
+def test_partition_units_spill_when_tables_run_out(monkeypatch, slot_table, kdt):
     # A group bound of 2^10 with 16 partitions sizes the unit tables for ~64
     # groups per partition; each partition holds ~2048.  The dense-id kernel
     # runs out of ids (the slot-indexed one closes its table): the remaining
@@ -181,7 +182,7 @@ def test_partition_units_spill_when_tables_run_out(monkeypatch, slot_table):
     if slot_table:
         monkeypatch.setenv("GX_UNITS_SLOT_TABLE", "1")
     n = 1 << 18
-    key = O.gen_keys(n, np.int32, groups=1 << 15, scatter=1, seed=23)
+    key = O.gen_keys(n, kdt, groups=1 << 15, scatter=1, seed=23)
     iv = O.gen_values(n, np.int64, lo=-(1 << 35), hi=1 << 35, seed=24)
     fv = O.gen_values(n, np.float64, seed=25)
     reqs = [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
@@ -274,9 +275,10 @@ def test_partition_min_max_monotone_values(order):
     assert_columns_match(got, exp)
 
 
+@pytest.mark.parametrize("kdt", [np.int32, np.int64])
 @pytest.mark.parametrize("slot_table", [False, True])
 @pytest.mark.parametrize("pattern", ["late_extremes", "decreasing"])
-def test_partition_min_max_large_units(monkeypatch, pattern, slot_table):
+def test_partition_min_max_large_units(monkeypatch, pattern, slot_table, kdt):
     # Units of ~56K rows (2^26 rows, 2^12 groups), through the dense-id unit
     # kernel and the slot-indexed one (GX_UNITS_SLOT_TABLE).
     # "late_extremes" plants every group's true MIN and MAX (and float NaN,
@@ -286,7 +288,7 @@ def test_partition_min_max_large_units(monkeypatch, pattern, slot_table):
     if slot_table:
         monkeypatch.setenv("GX_UNITS_SLOT_TABLE", "1")
     n, G = 1 << 26, 1 << 12
-    key = O.gen_keys(n, np.int32, groups=G, scatter=1, seed=43)
+    key = O.gen_keys(n, kdt, groups=G, scatter=1, seed=43)
     idx = np.arange(n, dtype=np.int64)
     if pattern == "decreasing":
         iv = (n - idx) * 7 - (1 << 33)
