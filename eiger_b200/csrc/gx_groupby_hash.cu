@@ -590,7 +590,10 @@ __device__ __forceinline__ unsigned long long ud_word(uint32_t tag, uint32_t id)
 }
 
 // Group id of key k (canonical; tag = the key itself for 4-byte keys, its
-// 32-bit hash for 8-byte ones), inserting it; UD_SPILL when the wait, the
+// 32-bit hash for 8-byte ones), inserting it.  Returns UD_PENDING when the
+// key's slot is claimed but not yet published (or, for 8-byte keys, its id's
+// key is not yet visible) instead of waiting: the inserter may be a lane of
+// the same warp, which a spinning branch can hold back.  UD_SPILL when the
 // ids or the probe walk run out.
 template <int KW>
 __device__ __forceinline__ uint32_t d_find_or_insert(const dtable<KW>& t, uint64_t k, uint32_t tag, uint32_t h) {
@@ -609,19 +612,32 @@ __device__ __forceinline__ uint32_t d_find_or_insert(const dtable<KW>& t, uint64
             }
         }
         if (ud_tag<KW>(cur) == tag) {
-            uint32_t g = ud_id<KW>(cur);
-            for (uint32_t w = 0; g == UD_PENDING && w < UD_WAIT_LIMIT; ++w) g = ud_id<KW>(ld_slot<KW>(&t.slots[slot]));
-            if (g == UD_PENDING || g == UD_SPILL) return UD_SPILL;
+            const uint32_t g = ud_id<KW>(cur);
+            if (g == UD_PENDING || g == UD_SPILL) return g;
             if (KW == 4) return g;
-            const volatile unsigned long long* gk = reinterpret_cast<volatile unsigned long long*>(t.gkey) + g;
-            unsigned long long kk = *gk;
-            for (uint32_t w = 0; kk == UD_UNSET && w < UD_WAIT_LIMIT; ++w) kk = *gk;
-            if (kk == UD_UNSET) return UD_SPILL;
+            const unsigned long long kk = reinterpret_cast<volatile unsigned long long*>(t.gkey)[g];
+            if (kk == UD_UNSET) return UD_PENDING;
             if (kk == k) return g;
         }
         slot = (slot + 1) & t.mask;
     }
     return UD_SPILL;
+}
+
+// d_find_or_insert for the live lanes of a whole warp (every lane calls it):
+// lanes that meet a pending slot retry after the warp regroups, so an
+// inserter in the same warp has published; after UD_WAIT_LIMIT rounds they
+// get UD_SPILL (their rows go to the global table).  Non-live lanes return
+// UD_SPILL.
+template <int KW>
+__device__ __forceinline__ uint32_t d_find_or_insert_warp(const dtable<KW>& t, bool live, uint64_t k, uint32_t tag,
+                                                          uint32_t h) {
+    uint32_t g = live ? d_find_or_insert<KW>(t, k, tag, h) : UD_SPILL;
+    for (uint32_t round = 0; __any_sync(0xffffffffu, g == UD_PENDING); ++round) {
+        __syncwarp();
+        if (g == UD_PENDING) g = round < UD_WAIT_LIMIT ? d_find_or_insert<KW>(t, k, tag, h) : UD_SPILL;
+    }
+    return g;
 }
 
 template <int KW>
@@ -698,7 +714,7 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const void* __restric
                 for (int c = 0; c < NV; ++c) vq[c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
             }
             const uint32_t hq = live ? key_hash<KW>(kq) : 0u;
-            const uint32_t gq = live ? d_find_or_insert<KW>(t, kq, tag_of(kq, hq), hq >> shift) : UD_SPILL;
+            const uint32_t gq = d_find_or_insert_warp<KW>(t, live, kq, tag_of(kq, hq), hq >> shift);
             __syncwarp();
             if (!live) return;
             if (gq < gcap) {
