@@ -88,18 +88,20 @@ struct char_span {
 };
 
 // An aligned word that reaches outside the span, assembled from its in-range
-// bytes (kept out of line: it is the rare edge of a column).
-__device__ __noinline__ uint64_t word_at_edge(const char_span& c, int64_t a) {
+// bytes (kept out of line: it is the rare edge of a column).  The span comes
+// in by value: a reference would make every caller keep its span in local
+// memory.
+__device__ __noinline__ uint64_t word_at_edge(const unsigned char* chars, int64_t lo, int64_t hi, int64_t a) {
     uint64_t w = 0;
     for (int k = 0; k < 8; ++k)
-        if (a + k >= c.lo && a + k < c.hi) w |= (uint64_t)c.chars[a + k] << (8 * k);
+        if (a + k >= lo && a + k < hi) w |= (uint64_t)chars[a + k] << (8 * k);
     return w;
 }
 
 __device__ __forceinline__ uint64_t word_at(const char_span& c, int64_t a) {
     // a: position (relative to chars) of an 8-byte-aligned address
     if (a >= c.lo && a + 8 <= c.hi) return __ldg(reinterpret_cast<const unsigned long long*>(c.chars + a));
-    return word_at_edge(c, a);
+    return word_at_edge(c.chars, c.lo, c.hi, a);
 }
 
 // The first min(len, 32) bytes of the string at [pos, pos + len) as four
@@ -210,8 +212,12 @@ __device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst
     return -1;
 }
 
-__global__ void __launch_bounds__(256) k_batch_main(batch_dev b) {
+// Four 256-thread blocks per SM (at most 64 registers): the kernel waits on
+// dependent L2 accesses (offsets, string words, table entry, representative
+// row), so resident warps matter more than registers.
+__global__ void __launch_bounds__(256, 4) k_batch_main(batch_dev b) {
     __shared__ long long s_item;
+    __shared__ inst_dev s_in;
     for (;;) {
         if (threadIdx.x == 0) {
             unsigned long long w = atomicAdd(b.work_counter, 1ull);
@@ -222,7 +228,11 @@ __global__ void __launch_bounds__(256) k_batch_main(batch_dev b) {
         __syncthreads();
         if (w < 0) break;
         const work_item it = b.work[w];
-        const inst_dev in = b.inst[it.inst];
+        // The work item's instance stays in shared memory (read per use):
+        // held in registers it cost every thread ~20 of them.
+        if (threadIdx.x == 0) s_in = b.inst[it.inst];
+        __syncthreads();
+        const inst_dev& in = s_in;
         for (int64_t r = it.begin + threadIdx.x; r < it.end; r += blockDim.x) {
             bool ins;
             int64_t slot = find_or_insert(b, in, it.inst, r, &ins);
