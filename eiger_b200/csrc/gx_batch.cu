@@ -62,7 +62,9 @@ struct batch_dev {
     const work_item* work;
     int64_t n_work;
     unsigned long long* entries;  // [total slots]: tag << 40 | (row + 1); 0 = empty
-    unsigned* code_of_slot;
+    unsigned* code_of_slot;       // dictionary code of a slot, ~0u until published (see find_or_insert)
+    unsigned long long* ks_key;   // [total codes][4]: first 32 bytes of the code's string, zero padded
+    unsigned* ks_len;             // [total codes]: its length
     unsigned long long* sum_slot;
     unsigned long long* cnt_slot;
     unsigned* dict_size;          // per instance
@@ -176,6 +178,16 @@ __device__ __forceinline__ bool str_eq_chunks(const char_span& c, int64_t pa, in
 }
 
 // Find or insert row r's string; returns the slot (or -1 on a full table).
+//
+// A new slot's inserter takes the next dictionary code, writes the string's
+// first 32 bytes and length to the key store at that code, fences, and only
+// then publishes the code in code_of_slot.  A row whose tag matches compares
+// against the key store when the slot's code is published (one aligned
+// 32-byte read), and against the slot's representative row in the input
+// otherwise (or for the bytes past 32) — it never waits on an inserter.
+// Without KEYSTORE (the plain engine's encoder, which numbers the slots
+// itself) every compare reads the representative row.
+template <bool KEYSTORE>
 __device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst_dev& in, int inst_id, int64_t r,
                                                   bool* inserted) {
     *inserted = false;
@@ -192,18 +204,47 @@ __device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst
     unsigned long long* tab = b.entries + in.table_off;
     for (uint32_t p = 0; p <= mask; ++p) {
         unsigned long long e = ((volatile unsigned long long*)tab)[slot];
+        const unsigned code = KEYSTORE ? ((const volatile unsigned*)b.code_of_slot)[in.table_off + slot] : ~0u;
         if (e == 0) {
             unsigned long long old = atomicCAS(tab + slot, 0ull, (unsigned long long)mine);
             if (old == 0) {
                 *inserted = true;
+                if (!KEYSTORE) return in.table_off + slot;
+                const unsigned c = atomicAdd(&b.dict_size[inst_id], 1u);
+                if (c < b.max_distinct) {
+                    ulonglong2* k = reinterpret_cast<ulonglong2*>(b.ks_key + ((size_t)in.result_off + c) * 4);
+                    k[0] = make_ulonglong2(ch[0], ch[1]);
+                    k[1] = make_ulonglong2(ch[2], ch[3]);
+                    b.ks_len[in.result_off + c] = (unsigned)len;
+                    __threadfence();
+                }
+                ((volatile unsigned*)b.code_of_slot)[in.table_off + slot] = c;
                 return in.table_off + slot;
             }
             e = old;
         }
         if ((e >> 40) == tag) {
-            int64_t rr = (int64_t)(e & ROW_MASK) - 1;
-            if (str_eq_chunks(sp, in.offsets[rr], in.offsets[rr + 1] - in.offsets[rr], o0, len, ch))
-                return in.table_off + slot;
+            bool eq;
+            if (code < b.max_distinct) {
+                // Read at L2 (__ldcg): the key store is rewritten by every run
+                // of the plan, and an SM's L1 may still hold an earlier run's
+                // bytes at these addresses.
+                const ulonglong2* k = reinterpret_cast<const ulonglong2*>(b.ks_key + ((size_t)in.result_off + code) * 4);
+                const ulonglong2 k0 = __ldcg(k), k1 = __ldcg(k + 1);
+                eq = __ldcg(b.ks_len + in.result_off + code) == (unsigned)len && k0.x == ch[0] && k0.y == ch[1] &&
+                     k1.x == ch[2] && k1.y == ch[3];
+                if (eq && len > 32) {
+                    const int64_t rr = (int64_t)(e & ROW_MASK) - 1, pa = in.offsets[rr];
+                    for (int64_t i = 32; eq && i < len; i += 8) {
+                        const int nb = (int)(len - i < 8 ? len - i : 8);
+                        eq = chunk_at(sp, pa + i, nb) == chunk_at(sp, o0 + i, nb);
+                    }
+                }
+            } else {
+                const int64_t rr = (int64_t)(e & ROW_MASK) - 1;
+                eq = str_eq_chunks(sp, in.offsets[rr], in.offsets[rr + 1] - in.offsets[rr], o0, len, ch);
+            }
+            if (eq) return in.table_off + slot;
         }
         slot = (slot + 1) & mask;
     }
@@ -235,9 +276,8 @@ __global__ void __launch_bounds__(256, 4) k_batch_main(batch_dev b) {
         const inst_dev& in = s_in;
         for (int64_t r = it.begin + threadIdx.x; r < it.end; r += blockDim.x) {
             bool ins;
-            int64_t slot = find_or_insert(b, in, it.inst, r, &ins);
+            int64_t slot = find_or_insert<true>(b, in, it.inst, r, &ins);
             if (slot < 0) continue;
-            if (ins) b.code_of_slot[slot] = atomicAdd(&b.dict_size[it.inst], 1u);
             int32_t dt = in.date[r];
             if (dt >= in.lo && dt < in.hi) {
                 atomicAdd(&b.sum_slot[slot], (unsigned long long)in.amount[r]);
@@ -293,7 +333,7 @@ __device__ __forceinline__ int64_t enc_find(const enc_dev& e, int64_t r, bool in
     in.table_off = 0;
     in.clo = e.clo;
     in.chi = e.chi;
-    if (insert) return find_or_insert(b, in, 0, r, inserted);
+    if (insert) return find_or_insert<false>(b, in, 0, r, inserted);
     // lookup only: the insert pass has published every string
     *inserted = false;
     const char_span sp{reinterpret_cast<const unsigned char*>(e.chars), e.clo, e.chi};
@@ -397,7 +437,7 @@ struct gx_batch_plan {
     uint32_t slots = 0;
     int tile_rows = 4096;
     int lf_pct = 50;
-    gx::dbuf d_inst, d_work, entries, code_of_slot, sum_slot, cnt_slot, dict_size, ctrl;
+    gx::dbuf d_inst, d_work, entries, code_of_slot, sum_slot, cnt_slot, dict_size, ctrl, ks_key, ks_len;
     gx::dbuf out_sum, out_cnt, out_first, out_groups;
     int64_t n_work = 0;
     cudaGraphExec_t graph = nullptr;
@@ -453,6 +493,8 @@ static void batch_layout(gx_batch_plan* p, int tile, int lf, cudaStream_t s) {
     p->out_cnt = dbuf(std::max<size_t>(total_codes, 1) * 8, s);
     p->out_first = dbuf(std::max<size_t>(total_codes, 1) * 8, s);
     p->out_groups = dbuf((size_t)std::max(n, 1) * 8, s);
+    p->ks_key = dbuf(std::max<size_t>(total_codes, 1) * 32, s);
+    p->ks_len = dbuf(std::max<size_t>(total_codes, 1) * 4, s);
     GX_CUDA(cudaStreamSynchronize(s));
     if (p->graph) {
         cudaGraphExecDestroy(p->graph);
@@ -470,6 +512,8 @@ static batch_dev batch_view(gx_batch_plan* p) {
     b.sum_slot = p->sum_slot.get<unsigned long long>();
     b.cnt_slot = p->cnt_slot.get<unsigned long long>();
     b.dict_size = p->dict_size.get<unsigned>();
+    b.ks_key = p->ks_key.get<unsigned long long>();
+    b.ks_len = p->ks_len.get<unsigned>();
     b.work_counter = p->ctrl.get<unsigned long long>();
     b.overflow = reinterpret_cast<int*>(p->ctrl.get<char>() + 8);
     b.slots = p->slots;
@@ -486,6 +530,7 @@ static void batch_enqueue(gx_batch_plan* p, cudaStream_t s, bool count_launches 
     const int n = (int)p->inst.size();
     const size_t total_slots = (size_t)n * p->slots, total_codes = (size_t)n * p->max_distinct;
     GX_CUDA(cudaMemsetAsync(p->entries.get(), 0, total_slots * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->code_of_slot.get(), 0xFF, total_slots * 4, s));
     GX_CUDA(cudaMemsetAsync(p->sum_slot.get(), 0, total_slots * 8, s));
     GX_CUDA(cudaMemsetAsync(p->cnt_slot.get(), 0, total_slots * 8, s));
     GX_CUDA(cudaMemsetAsync(p->dict_size.get(), 0, (size_t)n * 4, s));

@@ -28,6 +28,20 @@ def test_batched_and_plain_match_oracle():
     assert plan.results() == exp
 
 
+def test_repeated_runs_of_one_plan():
+    # Every run renumbers the strings (codes follow insertion order) and
+    # rewrites the key store at the same addresses; a lookup must never
+    # compare against bytes an earlier run left there (that inserts the
+    # string again, and max_distinct = the dictionary size turns any second
+    # insert into an overflow error).
+    insts, _ = B.make_instances(64, seed=11, min_log2=12, max_log2=17, dict_size=3000)
+    exp = expected(insts)
+    plan = B.Plan(insts, max_distinct=3000)
+    for _ in range(6):
+        plan.run()
+        assert plan.results() == exp
+
+
 def test_empty_and_tiny_instances():
     insts, _ = B.make_instances(5, seed=9, min_log2=0, max_log2=3, dict_size=50)
     plan = B.Plan(insts, max_distinct=50)
