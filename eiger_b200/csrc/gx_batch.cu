@@ -189,11 +189,9 @@ __device__ __forceinline__ bool str_eq_chunks(const char_span& c, int64_t pa, in
 // itself) every compare reads the representative row.
 template <bool KEYSTORE>
 __device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst_dev& in, int inst_id, int64_t r,
-                                                  bool* inserted) {
+                                                  int64_t o0, int64_t len, bool* inserted) {
     *inserted = false;
     const char_span sp{reinterpret_cast<const unsigned char*>(in.chars), in.clo, in.chi};
-    const int64_t o0 = in.offsets[r], o1 = in.offsets[r + 1];
-    const int64_t len = o1 - o0;
     uint64_t ch[4];
     load32(sp, o0, len, ch);
     const uint64_t h = str_hash_chunks(sp, o0, len, ch);
@@ -274,15 +272,37 @@ __global__ void __launch_bounds__(256, 4) k_batch_main(batch_dev b) {
         if (threadIdx.x == 0) s_in = b.inst[it.inst];
         __syncthreads();
         const inst_dev& in = s_in;
-        for (int64_t r = it.begin + threadIdx.x; r < it.end; r += blockDim.x) {
+        // A row's offsets, date and amount are loaded one iteration ahead,
+        // so the dependent chain of a row starts at its string bytes.
+        int64_t r = it.begin + threadIdx.x;
+        int64_t o0 = 0, o1 = 0, am = 0;
+        int32_t dt = 0;
+        if (r < it.end) {
+            o0 = in.offsets[r];
+            o1 = in.offsets[r + 1];
+            dt = in.date[r];
+            am = in.amount[r];
+        }
+        for (; r < it.end; r += blockDim.x) {
+            const int64_t rn = r + blockDim.x;
+            int64_t n0 = 0, n1 = 0, nam = 0;
+            int32_t ndt = 0;
+            if (rn < it.end) {
+                n0 = in.offsets[rn];
+                n1 = in.offsets[rn + 1];
+                ndt = in.date[rn];
+                nam = in.amount[rn];
+            }
             bool ins;
-            int64_t slot = find_or_insert<true>(b, in, it.inst, r, &ins);
-            if (slot < 0) continue;
-            int32_t dt = in.date[r];
-            if (dt >= in.lo && dt < in.hi) {
-                atomicAdd(&b.sum_slot[slot], (unsigned long long)in.amount[r]);
+            const int64_t slot = find_or_insert<true>(b, in, it.inst, r, o0, o1 - o0, &ins);
+            if (slot >= 0 && dt >= in.lo && dt < in.hi) {
+                atomicAdd(&b.sum_slot[slot], (unsigned long long)am);
                 atomicAdd(&b.cnt_slot[slot], 1ull);
             }
+            o0 = n0;
+            o1 = n1;
+            dt = ndt;
+            am = nam;
         }
     }
 }
@@ -333,7 +353,7 @@ __device__ __forceinline__ int64_t enc_find(const enc_dev& e, int64_t r, bool in
     in.table_off = 0;
     in.clo = e.clo;
     in.chi = e.chi;
-    if (insert) return find_or_insert<false>(b, in, 0, r, inserted);
+    if (insert) return find_or_insert<false>(b, in, 0, r, e.offsets[r], e.offsets[r + 1] - e.offsets[r], inserted);
     // lookup only: the insert pass has published every string
     *inserted = false;
     const char_span sp{reinterpret_cast<const unsigned char*>(e.chars), e.clo, e.chi};
