@@ -197,11 +197,13 @@ __global__ void __launch_bounds__(JP_NT) k_probe_write(build_run b, probe_side p
 
 template <int KW>
 __global__ void k_build_dir(const void* __restrict__ skeys, int64_t n, int kind, uint64_t lo, int shift,
-                            uint64_t nb, uint32_t* __restrict__ dir) {
+                            uint64_t nb, uint32_t* __restrict__ dir, int* __restrict__ dup) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x) {
-        uint64_t cur = i < n ? (img_of<KW>(skeys, i, kind) - lo) >> shift : nb;
-        uint64_t prev = i > 0 ? (img_of<KW>(skeys, i - 1, kind) - lo) >> shift : (uint64_t)-1;
+        const uint64_t ci = i < n ? img_of<KW>(skeys, i, kind) : 0, pi = i > 0 ? img_of<KW>(skeys, i - 1, kind) : 0;
+        uint64_t cur = i < n ? (ci - lo) >> shift : nb;
+        uint64_t prev = i > 0 ? (pi - lo) >> shift : (uint64_t)-1;
         for (uint64_t j = prev + 1; j <= cur; ++j) dir[j] = (uint32_t)i;
+        if (i > 0 && i < n && ci == pi) *dup = 1;  // equal neighbours: build keys are not unique
     }
 }
 
@@ -450,6 +452,76 @@ __global__ void __launch_bounds__(JP_NT) k_dense_probe1(const void* __restrict__
     }
 }
 
+// Single-pass probe of the sorted build run for unique build keys (at most
+// one match per probe row, so the outputs are allocated for every probe row
+// up front): the tile's matches are placed with the decoupled look-back of
+// k_dense_probe1 instead of a count kernel, a scan and a second lookup.
+template <int KW>
+__global__ void __launch_bounds__(JP_NT) k_sorted_probe1(build_run b, probe_side p, unsigned long long* __restrict__ tstate,
+                                                        unsigned* __restrict__ ticket, int64_t ntiles,
+                                                        int64_t* __restrict__ total_out, int* __restrict__ err,
+                                                        join_out o) {
+    __shared__ int64_t sm[JP_NT / 32 + 1];
+    __shared__ int64_t s_tile, s_excl;
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t row0 = tile * (int64_t)JP_TILE + warp * 32 * JP_IPT + lane;
+    uint64_t img[JP_IPT];
+    bool valid[JP_IPT];
+    int64_t first[JP_IPT];
+    int cnt[JP_IPT];
+    load_probe<KW>(p, row0, img, valid);
+    lookup_batch<KW, JP_IPT>(b, img, valid, first, cnt);
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) c += cnt[k] > 0;
+    const int64_t wtot = dev_::warp_sum((int64_t)c);
+    int64_t total;
+    int64_t wbase = dev_::block_exclusive_sum<JP_NT, int64_t>(lane == 0 ? wtot : 0, sm, &total);
+    if (warp == 0) {
+        const int64_t excl = lookback(tstate, tile, total, err);
+        __syncwarp();  // orders the lanes' acquire loads before lane 0 reads the error flag
+        if (lane == 0) {
+            s_excl = excl;
+            s_skip = *(volatile int*)err;
+            if (tile == ntiles - 1) *total_out = excl + total;
+        }
+    }
+    __syncthreads();
+    if (s_skip) return;  // block-uniform
+    wbase = __shfl_sync(0xffffffffu, wbase, 0) + s_excl;
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < JP_IPT; ++k) {
+        const bool hit = cnt[k] > 0;
+        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const int64_t pos = wbase + __popc(bal & lt);
+            const int64_t i = row0 + k * 32;
+            if (pos < p.n) {  // capacity bound (unique build keys never exceed it)
+                const int64_t bm = first[k];
+                const int64_t prow = p.rowid ? p.rowid[i] : i;
+                if (o.key) st_w(o.key, o.key_width, pos, ld_w(b.keys, o.key_width, bm));
+                for (int cc = 0; cc < o.n_pay; ++cc) {
+                    uint64_t v;
+                    switch (o.src[cc]) {
+                        case 0: v = ld_w(b.vals, b.val_width, bm); break;
+                        case 1: v = ld_w(o.col[cc], o.width[cc], (int64_t)ld_w(b.vals, 8, bm)); break;
+                        case 2: v = ld_w(o.col[cc], o.width[cc], prow); break;
+                        case 3: v = ld_w(b.vals, 8, bm); break;
+                        default: v = (uint64_t)prow; break;
+                    }
+                    st_w(o.out[cc], o.width[cc], pos, v);
+                }
+            }
+        }
+        wbase += __popc(bal);
+    }
+}
+
 // Output columns of a join: [key, left payloads.., right payloads..] or the
 // row-id pair; `dense` selects the source codes of the dense path.
 join_out make_outputs(const join_inputs& in, bool build_left, bool rowids_only, bool pay_in_run, bool dense,
@@ -605,10 +677,11 @@ static void join_core(const join_inputs& in, const gx_join_hint& hint, bool rowi
     int D = std::min(nbits, std::max(1, ilog2_ceil((uint64_t)std::max<int64_t>(nb, 2)) - 1));
     int shift = nbits - D;
     uint64_t nbk = (span >> shift) + 1;
-    dbuf dir((size_t)(nbk + 1) * 4, s);
+    dbuf dir((size_t)(nbk + 1) * 4, s), dup(8, s);
+    GX_CUDA(cudaMemsetAsync(dup.get(), 0, 8, s));
     if (nb > 0) {
-        if (kw == 4) k_build_dir<4><<<grid_for(nb + 1, 256, 8), 256, 0, s>>>(bk.get(), nb, kind, lo, shift, nbk, dir.get<uint32_t>());
-        else k_build_dir<8><<<grid_for(nb + 1, 256, 8), 256, 0, s>>>(bk.get(), nb, kind, lo, shift, nbk, dir.get<uint32_t>());
+        if (kw == 4) k_build_dir<4><<<grid_for(nb + 1, 256, 8), 256, 0, s>>>(bk.get(), nb, kind, lo, shift, nbk, dir.get<uint32_t>(), dup.get<int>());
+        else k_build_dir<8><<<grid_for(nb + 1, 256, 8), 256, 0, s>>>(bk.get(), nb, kind, lo, shift, nbk, dir.get<uint32_t>(), dup.get<int>());
         GX_LAUNCHED();
     }
     build_run br{bk.get(), bv.get(), vw, dir.get<uint32_t>(), nb, lo, hi, shift, kind};
@@ -629,6 +702,39 @@ static void join_core(const join_inputs& in, const gx_join_hint& hint, bool rowi
     }
 
     int64_t ntiles = ceil_div(std::max<int64_t>(np, 1), JP_TILE);
+    static const bool two_pass = getenv("GX_JOIN_TWO_PASS") != nullptr;
+    if (np > 0 && nb > 0 && !two_pass && !read_scalar(dup.get<int>(), s)) {
+        // Unique build keys: one probe pass, tiles placed by look-back.
+        dbuf tstate((size_t)ntiles * 8 + 16, s), scal(16, s);
+        GX_CUDA(cudaMemsetAsync(tstate.get(), 0, (size_t)ntiles * 8 + 16, s));
+        GX_CUDA(cudaMemsetAsync(scal.get(), 0, 16, s));
+        join_out o = make_outputs(in, build_left, rowids_only, pay_in_run, false, np, s, out, np);
+        unsigned* ticket = reinterpret_cast<unsigned*>(tstate.get<char>() + (size_t)ntiles * 8);
+        {
+            GX_PROF("join_probe_write", s);
+            if (kw == 4)
+                k_sorted_probe1<4><<<(unsigned)ntiles, JP_NT, 0, s>>>(br, ps, tstate.get<unsigned long long>(), ticket,
+                                                                     ntiles, scal.get<int64_t>(),
+                                                                     reinterpret_cast<int*>(scal.get<char>() + 8), o);
+            else
+                k_sorted_probe1<8><<<(unsigned)ntiles, JP_NT, 0, s>>>(br, ps, tstate.get<unsigned long long>(), ticket,
+                                                                     ntiles, scal.get<int64_t>(),
+                                                                     reinterpret_cast<int*>(scal.get<char>() + 8), o);
+            GX_LAUNCHED();
+        }
+        int64_t hs[2];
+        GX_CUDA(cudaMemcpyAsync(hs, scal.get(), 16, cudaMemcpyDeviceToHost, s));
+        GX_CUDA(cudaStreamSynchronize(s));
+        if ((int)hs[1] == 0) {
+            const int64_t total = hs[0];
+            if (hint.max_out > 0 && total > hint.max_out)
+                fail(GX_EOVERFLOW, "join output (" + std::to_string(total) + " rows) exceeds hint.max_out (" +
+                                       std::to_string(hint.max_out) + ")");
+            for (auto& c : out->cols) c.size = total;
+            return;
+        }
+        out->cols.clear();  // a look-back wait gave up: redo with the two-pass probe
+    }
     dbuf tc(ntiles * 8, s), toff((ntiles + 1) * 8, s);
     int64_t total = 0;
     if (np > 0 && nb > 0) {

@@ -113,6 +113,38 @@ def test_join_narrow_payload_layout(mode, mat):
     assert np.array_equal(key[o], bk[el])
 
 
+@pytest.mark.parametrize("two_pass", [False, True])
+@pytest.mark.parametrize("mode", [gx.SORTED_BUILD, gx.SORT_MERGE])
+@pytest.mark.parametrize("kdt", [np.int32, np.int64])
+def test_join_sparse_unique_build_single_pass(monkeypatch, mode, kdt, two_pass):
+    # Unique build keys spread 8 apart (too sparse for direct placement):
+    # the sorted-build and sort-merge matchers probe in one pass with the
+    # tiles placed by look-back (GX_JOIN_TWO_PASS: count, scan, write).
+    # Several tiles, a partial last tile, 10% absent probe keys, payloads of
+    # both sides and the row-id form.
+    if two_pass:
+        monkeypatch.setenv("GX_JOIN_TWO_PASS", "1")
+    nb, npr = 5000, 3 * 4096 + 777
+    bk = (O.gen_perm(nb, kdt, seed=21) * 8 - 40000).astype(kdt)
+    pick = O.gen_keys(npr, np.int64, groups=nb, seed=22)
+    pk = bk[pick].copy()
+    pk[::10] = 3  # 3 is not a multiple of 8 away from -40000: absent
+    bpay = O.gen_values(nb, np.float64, seed=23)
+    ppay = O.gen_values(npr, np.int32, lo=-5, hi=5, seed=24)
+    hint = gx.make_join_hint(gx.JOIN_SORT, gx.MAT_GFUR, sort_mode=mode)
+    t = gx.inner_eq_join([to_dev(bk), to_dev(bpay)], [to_dev(pk), to_dev(ppay)], hint)
+    key, c1, c2 = t.numpy_columns()
+    el, er = O.join_pairs(bk, pk)
+    exp = np.stack([bk[el].astype(np.int64), bpay[el].view(np.int64), ppay[er].astype(np.int64)])
+    got = np.stack([key.astype(np.int64), c1.view(np.int64), c2.astype(np.int64)])
+    assert got.shape == exp.shape
+    assert np.array_equal(got[:, np.lexsort(got[::-1])], exp[:, np.lexsort(exp[::-1])])
+    r = gx.inner_eq_join_rowids(to_dev(bk), to_dev(pk), hint)
+    l, p = r.numpy_columns()
+    o = np.lexsort((p, l))
+    assert np.array_equal(l[o], el) and np.array_equal(p[o], er)
+
+
 def test_join_many_to_many_and_wide_payloads():
     a = O.gen_keys(3000, np.int64, groups=500, seed=3)
     b = O.gen_keys(2000, np.int64, groups=700, seed=4)
