@@ -65,6 +65,7 @@ struct batch_dev {
     unsigned* code_of_slot;       // dictionary code of a slot, ~0u until published (see find_or_insert)
     unsigned long long* ks_key;   // [total codes][4]: first 32 bytes of the code's string, zero padded
     unsigned* ks_len;             // [total codes]: its length
+    unsigned* slot_of_code;       // [total codes]: the code's slot in its instance's table
     unsigned long long* sum_slot;
     unsigned long long* cnt_slot;
     unsigned* dict_size;          // per instance
@@ -214,6 +215,7 @@ __device__ __forceinline__ int64_t find_or_insert(const batch_dev& b, const inst
                     k[0] = make_ulonglong2(ch[0], ch[1]);
                     k[1] = make_ulonglong2(ch[2], ch[3]);
                     b.ks_len[in.result_off + c] = (unsigned)len;
+                    b.slot_of_code[in.result_off + c] = slot;
                     __threadfence();
                 }
                 ((volatile unsigned*)b.code_of_slot)[in.table_off + slot] = c;
@@ -307,24 +309,41 @@ __global__ void __launch_bounds__(256, 4) k_batch_main(batch_dev b) {
     }
 }
 
-// Per-code results from the slot tables (grid over all slots).
+// Per-code results (grid over all instances' codes): each code's slot gives
+// its first row, SUM and COUNT.  The finalize also returns the slots it read
+// to their empty state, so the next run of the plan starts from clean tables
+// without clearing every slot (after an overflow the host clears them all).
+// Lanes of a warp that share an instance add their kept groups with one
+// atomic.
 __global__ void k_batch_finalize(batch_dev b, int n_inst) {
-    const int64_t total = (int64_t)n_inst * b.slots;
-    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
-        unsigned long long e = b.entries[g];
-        if (e == 0) continue;
-        const int inst = (int)(g / b.slots);
-        const unsigned code = b.code_of_slot[g];
-        if (code >= b.max_distinct) {
-            atomicExch(b.overflow, 1);
-            continue;
+    const int64_t total = (int64_t)n_inst * b.max_distinct;
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < total; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = base + threadIdx.x;
+        int inst = -1;
+        bool kept = false;
+        if (o < total) {
+            inst = (int)(o / b.max_distinct);
+            const uint32_t code = (uint32_t)(o - (int64_t)inst * b.max_distinct);
+            const unsigned nd = b.dict_size[inst];
+            if (nd > b.max_distinct && code == 0) atomicExch(b.overflow, 1);
+            if (code < nd) {
+                const int64_t g = b.inst[inst].table_off + b.slot_of_code[o];
+                const unsigned long long c = b.cnt_slot[g];
+                b.out_sum[o] = (long long)b.sum_slot[g];
+                b.out_cnt[o] = (long long)c;
+                b.out_first[o] = (long long)(b.entries[g] & ROW_MASK) - 1;
+                kept = c != 0;
+                b.entries[g] = 0;
+                b.sum_slot[g] = 0;
+                b.cnt_slot[g] = 0;
+                b.code_of_slot[g] = ~0u;
+            }
         }
-        const int64_t o = b.inst[inst].result_off + code;
-        const unsigned long long c = b.cnt_slot[g];
-        b.out_sum[o] = (long long)b.sum_slot[g];
-        b.out_cnt[o] = (long long)c;
-        b.out_first[o] = (long long)(e & ROW_MASK) - 1;
-        if (c) atomicAdd((unsigned long long*)&b.out_groups[inst], 1ull);
+        const unsigned same = __match_any_sync(0xffffffffu, inst);
+        const unsigned hits = __ballot_sync(0xffffffffu, kept) & same;
+        if (inst >= 0 && hits && lane == __ffs(same) - 1)
+            atomicAdd((unsigned long long*)&b.out_groups[inst], (unsigned long long)__popc(hits));
     }
 }
 
@@ -457,7 +476,7 @@ struct gx_batch_plan {
     uint32_t slots = 0;
     int tile_rows = 4096;
     int lf_pct = 50;
-    gx::dbuf d_inst, d_work, entries, code_of_slot, sum_slot, cnt_slot, dict_size, ctrl, ks_key, ks_len;
+    gx::dbuf d_inst, d_work, entries, code_of_slot, sum_slot, cnt_slot, dict_size, ctrl, ks_key, ks_len, slot_of_code;
     gx::dbuf out_sum, out_cnt, out_first, out_groups;
     int64_t n_work = 0;
     cudaGraphExec_t graph = nullptr;
@@ -470,6 +489,15 @@ struct gx_batch_plan {
 };
 
 namespace gx {
+
+// Every slot empty: entry 0, no code, zero SUM and COUNT.
+static void clear_tables(gx_batch_plan* p, cudaStream_t s) {
+    const size_t total_slots = p->inst.size() * (size_t)p->slots;
+    GX_CUDA(cudaMemsetAsync(p->entries.get(), 0, total_slots * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->code_of_slot.get(), 0xFF, total_slots * 4, s));
+    GX_CUDA(cudaMemsetAsync(p->sum_slot.get(), 0, total_slots * 8, s));
+    GX_CUDA(cudaMemsetAsync(p->cnt_slot.get(), 0, total_slots * 8, s));
+}
 
 static void batch_layout(gx_batch_plan* p, int tile, int lf, cudaStream_t s) {
     const int n = (int)p->inst.size();
@@ -515,6 +543,8 @@ static void batch_layout(gx_batch_plan* p, int tile, int lf, cudaStream_t s) {
     p->out_groups = dbuf((size_t)std::max(n, 1) * 8, s);
     p->ks_key = dbuf(std::max<size_t>(total_codes, 1) * 32, s);
     p->ks_len = dbuf(std::max<size_t>(total_codes, 1) * 4, s);
+    p->slot_of_code = dbuf(std::max<size_t>(total_codes, 1) * 4, s);
+    clear_tables(p, s);
     GX_CUDA(cudaStreamSynchronize(s));
     if (p->graph) {
         cudaGraphExecDestroy(p->graph);
@@ -534,6 +564,7 @@ static batch_dev batch_view(gx_batch_plan* p) {
     b.dict_size = p->dict_size.get<unsigned>();
     b.ks_key = p->ks_key.get<unsigned long long>();
     b.ks_len = p->ks_len.get<unsigned>();
+    b.slot_of_code = p->slot_of_code.get<unsigned>();
     b.work_counter = p->ctrl.get<unsigned long long>();
     b.overflow = reinterpret_cast<int*>(p->ctrl.get<char>() + 8);
     b.slots = p->slots;
@@ -548,11 +579,9 @@ static batch_dev batch_view(gx_batch_plan* p) {
 // The whole batched run as stream work (resets, main, finalize).
 static void batch_enqueue(gx_batch_plan* p, cudaStream_t s, bool count_launches = true) {
     const int n = (int)p->inst.size();
-    const size_t total_slots = (size_t)n * p->slots, total_codes = (size_t)n * p->max_distinct;
-    GX_CUDA(cudaMemsetAsync(p->entries.get(), 0, total_slots * 8, s));
-    GX_CUDA(cudaMemsetAsync(p->code_of_slot.get(), 0xFF, total_slots * 4, s));
-    GX_CUDA(cudaMemsetAsync(p->sum_slot.get(), 0, total_slots * 8, s));
-    GX_CUDA(cudaMemsetAsync(p->cnt_slot.get(), 0, total_slots * 8, s));
+    const size_t total_codes = (size_t)n * p->max_distinct;
+    // The slot tables are clean here: set up once by batch_layout and
+    // returned to empty by the previous run's finalize.
     GX_CUDA(cudaMemsetAsync(p->dict_size.get(), 0, (size_t)n * 4, s));
     GX_CUDA(cudaMemsetAsync(p->ctrl.get(), 0, 16, s));
     GX_CUDA(cudaMemsetAsync(p->out_sum.get(), 0, total_codes * 8, s));
@@ -562,7 +591,7 @@ static void batch_enqueue(gx_batch_plan* p, cudaStream_t s, bool count_launches 
     batch_dev b = batch_view(p);
     k_batch_main<<<dev().sm_count * 8, 256, 0, s>>>(b);
     GX_CUDA(cudaGetLastError());
-    k_batch_finalize<<<grid_for((int64_t)total_slots, 256, 8), 256, 0, s>>>(b, n);
+    k_batch_finalize<<<grid_for((int64_t)std::max<size_t>(total_codes, 1), 256, 8), 256, 0, s>>>(b, n);
     GX_CUDA(cudaGetLastError());
     if (count_launches) g_launches.fetch_add(2);
 }
@@ -604,7 +633,12 @@ static void batch_autotune(gx_batch_plan* p, cudaStream_t s) {
 
 static void check_overflow(gx_batch_plan* p, cudaStream_t s) {
     int ovf = read_scalar(reinterpret_cast<int*>(p->ctrl.get<char>() + 8), s);
-    if (ovf) fail(GX_EOVERFLOW, "batch: an instance exceeded max_distinct or its table filled");
+    if (ovf) {
+        // Slots past max_distinct were never listed for the finalize to clear.
+        clear_tables(p, s);
+        GX_CUDA(cudaStreamSynchronize(s));
+        fail(GX_EOVERFLOW, "batch: an instance exceeded max_distinct or its table filled");
+    }
 }
 
 static void batch_run(gx_batch_plan* p, cudaStream_t s) {
