@@ -145,6 +145,26 @@ def test_join_sparse_unique_build_single_pass(monkeypatch, mode, kdt, two_pass):
     assert np.array_equal(l[o], el) and np.array_equal(p[o], er)
 
 
+def test_join_dense_build_with_gaps():
+    # Unique build keys covering 3/4 of their range (direct placement with
+    # empty positions) and, with SORTED_BUILD, the sorted-build matcher.
+    # Probe keys hit, fall into gaps and fall outside the range; several
+    # tiles and a partial last one.
+    span = 40000
+    rng = np.random.default_rng(31)
+    bk = rng.permutation(span)[: span * 3 // 4].astype(np.int32) - 1000
+    npr = 5 * 4096 + 123
+    pk = rng.integers(-3000, span + 2000, npr).astype(np.int32)
+    for hint in (gx.make_join_hint(gx.JOIN_SORT, gx.MAT_GFUR),
+                 gx.make_join_hint(gx.JOIN_SORT, gx.MAT_GFUR, sort_mode=gx.SORTED_BUILD)):
+        t = gx.inner_eq_join_rowids(to_dev(bk), to_dev(pk), hint)
+        l, p = t.numpy_columns()
+        o = np.lexsort((p, l))
+        el, er = O.join_pairs(bk, pk)
+        assert len(el) > npr // 3
+        assert np.array_equal(l[o], el) and np.array_equal(p[o], er)
+
+
 def test_join_many_to_many_and_wide_payloads():
     a = O.gen_keys(3000, np.int64, groups=500, seed=3)
     b = O.gen_keys(2000, np.int64, groups=700, seed=4)
