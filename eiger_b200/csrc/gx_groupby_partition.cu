@@ -969,18 +969,25 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
 
     uint64_t empty = kw == 4 ? PG_EMPTY4 : PG_EMPTY8;
     // Split units merge through the spill table, so size it for every group
-    // when any partition was split; otherwise it only catches overflow.
-    int64_t tail[2];
-    GX_CUDA(cudaMemcpyAsync(tail, uoff.get<int64_t>() + P, sizeof(tail), cudaMemcpyDeviceToHost, s));
-    GX_CUDA(cudaStreamSynchronize(s));
-    const int64_t total_units = tail[0];
-    if ((int)tail[1]) fail(GX_ETIMEOUT, "partition scatter: a bulk copy into shared memory did not complete");
-    int64_t live_parts = std::min<int64_t>(P, n);
+    // when any partition was split; otherwise it only catches overflow.  When
+    // a table for every group is small (<= 64 MB) it is used either way, so
+    // the host does not wait for the unit count before the aggregation; the
+    // scatter's timeout flag is then read with the final flags.
+    int64_t tail[2] = {0, 0};
+    const int64_t live_parts = std::min<int64_t>(P, n);
+    const uint64_t all_groups = std::max<uint64_t>(1u << 16, next_pow2((uint64_t)bound * 2));
     uint64_t gcap = 1u << 16;
-    // Also when partitions hold more groups than a shared table (radix bits
-    // forced low by the hint): their overflow spills here.
-    if (total_units > live_parts || ceil_div(bound, (int64_t)P) > 512)
-        gcap = std::max<uint64_t>(gcap, next_pow2((uint64_t)bound * 2));
+    const bool tail_later = (all_groups + 1) * (uint64_t)d.rec_words * 8 <= (64ull << 20);
+    if (tail_later) {
+        gcap = all_groups;
+    } else {
+        GX_CUDA(cudaMemcpyAsync(tail, uoff.get<int64_t>() + P, sizeof(tail), cudaMemcpyDeviceToHost, s));
+        GX_CUDA(cudaStreamSynchronize(s));
+        if ((int)tail[1]) fail(GX_ETIMEOUT, "partition scatter: a bulk copy into shared memory did not complete");
+        // Also when partitions hold more groups than a shared table (radix
+        // bits forced low by the hint): their overflow spills here.
+        if (tail[0] > live_parts || ceil_div(bound, (int64_t)P) > 512) gcap = all_groups;
+    }
     int64_t out_cap = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
     // Output records: sized from the group bound, grown (up to n) on overflow.
     int64_t rec_cap = std::max<int64_t>(1, std::min<int64_t>(n, std::max<int64_t>(bound + bound / 4, 4096)));
@@ -1035,7 +1042,10 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
         GX_LAUNCHED();
         int fl[8];
         GX_CUDA(cudaMemcpyAsync(fl, flags.get(), sizeof(fl), cudaMemcpyDeviceToHost, s));
+        if (tail_later) GX_CUDA(cudaMemcpyAsync(tail, uoff.get<int64_t>() + P, sizeof(tail), cudaMemcpyDeviceToHost, s));
         GX_CUDA(cudaStreamSynchronize(s));
+        if (tail_later && (int)tail[1])
+            fail(GX_ETIMEOUT, "partition scatter: a bulk copy into shared memory did not complete");
         if (fl[1]) { gcap *= 8; continue; }
         unsigned long long ocount_h;
         std::memcpy(&ocount_h, reinterpret_cast<const char*>(fl) + 8, 8);

@@ -192,23 +192,45 @@ void selector_features(const col& key_in, float* f, cudaStream_t s) {
     radix_sort(sc, nullptr, 0, false, 0, size_of(key.type) == 8 ? -1 : 32, false, sorted.get(), nullptr, nullptr, 0,
                s);
     hll_registers(key, m, stride, regs.get<unsigned>(), s);
-    std::vector<uint64_t> h(m);
-    std::vector<unsigned> hr(8192);
-    GX_CUDA(cudaMemcpyAsync(h.data(), sorted.get(), (size_t)m * 8, cudaMemcpyDeviceToHost, s));
-    GX_CUDA(cudaMemcpyAsync(hr.data(), regs.get(), 8192 * 4, cudaMemcpyDeviceToHost, s));
+    // Pinned host staging (one buffer per host thread, kept): a pageable
+    // destination would make the driver bounce the copy through its own.
+    struct pinned_sample {
+        void* p = nullptr;
+        ~pinned_sample() {
+            if (p) cudaFreeHost(p);
+        }
+    };
+    static thread_local pinned_sample stage;
+    if (!stage.p) GX_CUDA(cudaMallocHost(&stage.p, (size_t)GX_SEL_SAMPLE_ROWS * 8 + 8192 * 4));
+    const uint64_t* h = static_cast<const uint64_t*>(stage.p);
+    const unsigned* hr = reinterpret_cast<const unsigned*>(static_cast<char*>(stage.p) + (size_t)GX_SEL_SAMPLE_ROWS * 8);
+    GX_CUDA(cudaMemcpyAsync(stage.p, sorted.get(), (size_t)m * 8, cudaMemcpyDeviceToHost, s));
+    GX_CUDA(cudaMemcpyAsync(static_cast<char*>(stage.p) + (size_t)GX_SEL_SAMPLE_ROWS * 8, regs.get(), 8192 * 4,
+                            cudaMemcpyDeviceToHost, s));
     GX_CUDA(cudaStreamSynchronize(s));
-    std::vector<int64_t> runs;
-    int64_t f1 = 0;
+    // Runs of equal keys in the sorted sample: their count, the singletons
+    // and the eight longest (kept in order while scanning; the device waits
+    // for this, so no full sort of ~m run lengths).
+    int64_t top[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t f1 = 0, nruns = 0;
     for (int64_t i = 0; i < m;) {
         int64_t j = i + 1;
         while (j < m && h[j] == h[i]) ++j;
-        runs.push_back(j - i);
-        f1 += (j - i) == 1;
+        const int64_t len = j - i;
+        ++nruns;
+        f1 += len == 1;
+        if (len > top[7]) {
+            int t = 7;
+            while (t > 0 && top[t - 1] < len) {
+                top[t] = top[t - 1];
+                --t;
+            }
+            top[t] = len;
+        }
         i = j;
     }
-    std::sort(runs.begin(), runs.end(), std::greater<int64_t>());
-    const double d = (double)runs.size();
-    const double hll = hll_estimate(hr.data());
+    const double d = (double)nruns;
+    const double hll = hll_estimate(hr);
     const double gee = std::sqrt((double)n / (double)m) * (double)f1 + (d - (double)f1);
     f[0] = (float)(std::log2((double)n) / 28.0);
     f[1] = size_of(key.type) == 8 ? 1.f : 0.f;
@@ -216,7 +238,7 @@ void selector_features(const col& key_in, float* f, cudaStream_t s) {
     f[3] = (float)(std::log2(1.0 + d) / 14.0);
     f[4] = (float)(d / (double)m);
     f[5] = (float)((double)f1 / (double)m);
-    for (int t = 0; t < 8; ++t) f[6 + t] = t < (int)runs.size() ? (float)((double)runs[t] / (double)m) : 0.f;
+    for (int t = 0; t < 8; ++t) f[6 + t] = (float)((double)top[t] / (double)m);
     f[14] = (float)(std::log2(1.0 + gee) / 28.0);
     f[15] = (float)(std::log2((double)n / std::max(1.0, gee)) / 28.0);
 }
