@@ -115,6 +115,15 @@ struct per_device_flag {
 // ---------------------------------------------------------------------------
 void* pool_alloc(size_t bytes, cudaStream_t s);
 void pool_free(void* p, cudaStream_t s);
+// A device buffer of at least `bytes` kept for the calling host thread
+// between library calls (one per device and slot), grown when a call needs
+// more; released when the thread exits.  For the large temporaries of one
+// call (the partitioned column copies, digit counts and group records of the
+// PARTITION plan): allocating them from the stream pool on every call stalled for up
+// to 20 ms while the pool grew.  Safe to reuse because every library call
+// returns after its device work is complete.
+void* thread_scratch(int slot, size_t bytes);
+constexpr int SCRATCH_SLOTS = 32;
 void pool_stats(int64_t* cur, int64_t* peak);
 void pool_reset_peak();
 

@@ -893,14 +893,15 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     // Partitioned copies.
     move_cols mc;
     std::memset(&mc, 0, sizeof(mc));
-    std::vector<dbuf> bufs_a, bufs_b;
+    // Partitioned copies (scratch slots 0..8 and, for a second pass, 9..17).
+    std::vector<void*> bufs_a, bufs_b;
     auto add_col = [&](const void* in, int w, int iota) {
         int c = mc.n++;
         mc.in[c] = in;
         mc.width[c] = w;
         mc.iota[c] = iota;
-        bufs_a.emplace_back((size_t)std::max<int64_t>(n, 1) * w, s);
-        mc.out[c] = bufs_a.back().get();
+        bufs_a.push_back(thread_scratch((int)bufs_a.size(), (size_t)std::max<int64_t>(n, 1) * w));
+        mc.out[c] = bufs_a.back();
     };
     // 1- and 2-byte value columns are read through row ids (GFUR) instead of
     // being moved by the 4/8-byte scatter.
@@ -911,7 +912,8 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
         for (int c = 0; c < d.n_cols; ++c) add_col(d.col_ptr[c], d.col_width[c], 0);
 
     int64_t ntiles = ceil_div(std::max<int64_t>(n, 1), PS_TILE);
-    dbuf counts((size_t)PS_BINS * ntiles * 8, s), offs((size_t)PS_BINS * ntiles * 8 + 8, s);
+    int64_t* counts = static_cast<int64_t*>(thread_scratch(SCRATCH_SLOTS - 2, (size_t)PS_BINS * ntiles * 8));
+    int64_t* offs = static_cast<int64_t*>(thread_scratch(SCRATCH_SLOTS - 1, (size_t)PS_BINS * ntiles * 8 + 8));
     // Unit offsets [0, P] then one word the bulk-copy scatter sets when a
     // copy wait gave up, so one read after the unit setup fetches both.
     dbuf uoff((size_t)(P + 2) * 8, s);
@@ -920,22 +922,23 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     int passes = (R + 7) / 8;
     // Two digit passes ping-pong between bufs_a and bufs_b.
     if (passes == 2)
-        for (int c = 0; c < mc.n; ++c) bufs_b.emplace_back((size_t)std::max<int64_t>(n, 1) * mc.width[c], s);
+        for (int c = 0; c < mc.n; ++c)
+            bufs_b.push_back(thread_scratch(MAX_VCOLS + 1 + c, (size_t)std::max<int64_t>(n, 1) * mc.width[c]));
     if (n > 0) {
         int shift = 0;
         for (int ps = 0; ps < passes; ++ps) {
             int dbits = std::min(8, R - shift);
             move_cols m = mc;
             if (passes == 2 && ps == 0) {
-                for (int c = 0; c < mc.n; ++c) m.out[c] = bufs_b[c].get();
+                for (int c = 0; c < mc.n; ++c) m.out[c] = bufs_b[c];
             } else if (passes == 2 && ps == 1) {
-                for (int c = 0; c < mc.n; ++c) { m.in[c] = bufs_b[c].get(); m.iota[c] = 0; m.out[c] = bufs_a[c].get(); }
+                for (int c = 0; c < mc.n; ++c) { m.in[c] = bufs_b[c]; m.iota[c] = 0; m.out[c] = bufs_a[c]; }
             }
             const void* kin = m.in[0];
             // Only the first digit pass may leave rows unordered within a run.
             const bool stable = ps > 0;
-            if (kw == 4) part_pass<4>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr, stable, s);
-            else part_pass<8>(kin, n, kind, shift, dbits, m, counts.get<int64_t>(), offs.get<int64_t>(), perr, stable, s);
+            if (kw == 4) part_pass<4>(kin, n, kind, shift, dbits, m, counts, offs, perr, stable, s);
+            else part_pass<8>(kin, n, kind, shift, dbits, m, counts, offs, perr, stable, s);
             shift += dbits;
         }
     }
@@ -945,7 +948,7 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
     if (passes == 1 && n > 0) {
         // One pass: the scanned digit counts already hold each partition's
         // start (bin p's offset in the first tile).
-        k_starts_from_offsets<<<(unsigned)ceil_div(P + 1, 256), 256, 0, s>>>(offs.get<int64_t>(), ntiles, P, n,
+        k_starts_from_offsets<<<(unsigned)ceil_div(P + 1, 256), 256, 0, s>>>(offs, ntiles, P, n,
                                                                             pstart.get<int64_t>());
         GX_LAUNCHED();
     } else {
@@ -996,7 +999,7 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
         dbuf flags(32, s);  // [0] sentinel, [1] spill overflow, [8..15] count, [16] record overflow
         GX_CUDA(cudaMemsetAsync(flags.get(), 0, 32, s));
         init_records(grec.get<uint64_t>(), (int64_t)gcap + 1, d, empty, s);
-        dbuf orec((size_t)rec_cap * d.rec_words * 8, s);
+        uint64_t* orec = static_cast<uint64_t*>(thread_scratch(SCRATCH_SLOTS - 3, (size_t)rec_cap * d.rec_words * 8));
         unsigned long long* ocount = reinterpret_cast<unsigned long long*>(flags.get<char>() + 8);
         int* rec_ovf = reinterpret_cast<int*>(flags.get<char>() + 16);
         pglobal g{grec.get<uint64_t>(), gcap - 1, flags.get<int>(), flags.get<int>() + 1};
@@ -1008,7 +1011,7 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
             for (int c = 0; c < d.n_cols; ++c) pd.col_ptr[c] = mc.out[c + 1];
             done_units = hash_units_aggregate(mc.out[0], kw, kind, pd, units.get<part_unit>(), uoff.get<int64_t>() + P,
                                               ceil_div(bound, (int64_t)P), R, grec.get<uint64_t>(), gcap,
-                                              flags.get<int>(), orec.get<uint64_t>(), ocount, rec_cap, rec_ovf, s);
+                                              flags.get<int>(), orec, ocount, rec_cap, rec_ovf, s);
         }
         if (n > 0 && !done_units) {
             size_t smem = (size_t)S * per_slot;
@@ -1023,12 +1026,12 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
             if (kw == 4) {
                 GX_CUDA(cudaFuncSetAttribute(k_part_agg<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 k_part_agg<4><<<grid, PA_NT, smem, s>>>(mc.out[0], prow, pv, kind, d, units.get<unit>(),
-                                                       uoff.get<int64_t>() + P, S, R, g, orec.get<uint64_t>(), ocount,
+                                                       uoff.get<int64_t>() + P, S, R, g, orec, ocount,
                                                        rec_cap, rec_ovf);
             } else {
                 GX_CUDA(cudaFuncSetAttribute(k_part_agg<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 k_part_agg<8><<<grid, PA_NT, smem, s>>>(mc.out[0], prow, pv, kind, d, units.get<unit>(),
-                                                       uoff.get<int64_t>() + P, S, R, g, orec.get<uint64_t>(), ocount,
+                                                       uoff.get<int64_t>() + P, S, R, g, orec, ocount,
                                                        rec_cap, rec_ovf);
             }
             GX_LAUNCHED();
@@ -1037,7 +1040,7 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
         // so one read decides: a spill-table overflow discards this attempt.
         k_append_global<<<grid_for((int64_t)gcap + 1, 256, 4), 256, 0, s>>>(grec.get<uint64_t>(), (int64_t)gcap,
                                                                           d.rec_words, empty, flags.get<int>(),
-                                                                          orec.get<uint64_t>(), ocount, rec_cap,
+                                                                          orec, ocount, rec_cap,
                                                                           rec_ovf);
         GX_LAUNCHED();
         int fl[8];
@@ -1054,7 +1057,7 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
             rec_cap = std::min<int64_t>(std::max<int64_t>(n, 1), rec_cap * 4);
             continue;
         }
-        emit_groupby_output(p, orec.get<uint64_t>(), groups, false, 0, -1, nullptr, key_in.type, out_cap, s, out);
+        emit_groupby_output(p, orec, groups, false, 0, -1, nullptr, key_in.type, out_cap, s, out);
         return;
     }
     fail(GX_EOVERFLOW, "partition group-by spill table overflow after retries");

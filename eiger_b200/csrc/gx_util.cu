@@ -113,6 +113,47 @@ void* pool_alloc(size_t bytes, cudaStream_t s) {
     return p;
 }
 
+namespace {
+struct scratch_set {
+    struct buf {
+        void* p = nullptr;
+        size_t bytes = 0;
+        int device = -1;
+    };
+    buf b[GX_MAX_DEVICES][SCRATCH_SLOTS];
+    ~scratch_set() {
+        for (auto& d : b)
+            for (auto& x : d)
+                if (x.p) {
+                    cudaSetDevice(x.device);
+                    cudaFree(x.p);  // errors ignored: the context may already be gone at exit
+                }
+    }
+};
+thread_local scratch_set t_scratch;
+}  // namespace
+
+void* thread_scratch(int slot, size_t bytes) {
+    require(slot >= 0 && slot < SCRATCH_SLOTS, "scratch slot out of range");
+    const int d = dev().device;
+    auto& x = t_scratch.b[d][slot];
+    if (x.bytes < bytes) {
+        if (x.p) GX_CUDA(cudaFree(x.p));
+        x.p = nullptr;
+        x.bytes = 0;
+        const size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&x.p, want);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            fail(GX_ENOMEM, "device memory exhausted allocating " + std::to_string(bytes) + " bytes of scratch");
+        }
+        GX_CUDA(e);
+        x.bytes = want;
+        x.device = d;
+    }
+    return x.p;
+}
+
 void pool_free(void* p, cudaStream_t s) {
     if (!p) return;
     size_t n = 0;
