@@ -129,9 +129,10 @@ __device__ __forceinline__ int s_find_or_insert(const stable<KW>& t, uint64_t kw
 
 constexpr int HGB_NT = 1024;
 constexpr int HGB_UNROLL = 4;
-// Rows per thread per batch in the unit kernel: two measured best (7
-// aggregates at 2^28 rows: 3.26 ms against 3.44 ms with four).
-constexpr int HU_UNROLL = 2;
+// Rows per thread per batch in the unit kernels: three measured best for the
+// dense-id kernel (7 aggregates at 2^28 rows, 2^16 groups: 2.52 ms against
+// 2.60 with two and 2.98 with four).
+constexpr int HU_UNROLL = 3;
 
 template <int KW, bool SMEM, int NV, class... ACCS>
 __global__ void __launch_bounds__(HGB_NT, 1) k_hash_groupby(const void* __restrict__ keys, int64_t n,
