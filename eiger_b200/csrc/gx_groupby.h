@@ -23,9 +23,12 @@ struct part_unit {
 // appended to orec / *ocount; the rest merge into the global record table
 // grec (gcap records + the sentinel record; gflags[0] sentinel, [1] overflow).
 // Returns false when the groups per partition do not fit a shared table.
+// dense_only: only the dense-id kernel (false when the plan has no compiled
+// form or its tables do not fit).
 bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d, const part_unit* units,
                           const int64_t* n_units, int64_t gpp, int shift, uint64_t* grec, uint64_t gcap, int* gflags,
-                          uint64_t* orec, unsigned long long* ocount, int64_t rec_cap, int* rec_ovf, cudaStream_t s);
+                          uint64_t* orec, unsigned long long* ocount, int64_t rec_cap, int* rec_ovf, cudaStream_t s,
+                          bool dense_only = false);
 void hash_groupby(const col& key, const agg_plan& p, gx_groupby_hint* hint, cudaStream_t s,
                   gx_table* out);
 

@@ -128,6 +128,7 @@ __device__ __forceinline__ int s_find_or_insert(const stable<KW>& t, uint64_t kw
 }
 
 constexpr int HGB_NT = 1024;
+constexpr int64_t HASH_UNITS_MAX_GROUPS = 4096;
 constexpr int HGB_UNROLL = 4;
 // Rows per thread per batch in the unit kernels: three measured best for the
 // dense-id kernel (7 aggregates at 2^28 rows, 2^16 groups: 2.52 ms against
@@ -1019,8 +1020,36 @@ static void units_dispatch(int grid, size_t smem, cudaStream_t s, const agg_desc
 
 // Runs the hash group-by into a global table of `cap` records.
 // Returns false when the table overflowed (caller retries larger).
+// HASH through the dense-id unit kernel for a few thousand groups at most:
+// the rows are cut into one range per SM, each a piece of one "partition"
+// holding every group, aggregated in the CTA's dense table (group ids,
+// replicated accumulators, no atomics on the global table per row) and
+// merged into the global table once per range.
+static bool hash_groupby_units(const col& key, const agg_desc& d, int64_t groups, const gtable& g, cudaStream_t s) {
+    const int64_t n = key.n;
+    const int ns = dev().sm_count;
+    std::vector<part_unit> hu;
+    const int64_t per = ceil_div(n, (int64_t)ns);
+    for (int64_t b = 0; b < n; b += per) hu.push_back({b, std::min(n, b + per), 1, 0});
+    const int64_t nu = (int64_t)hu.size();
+    dbuf ub((size_t)nu * sizeof(part_unit) + 64, s);
+    int64_t* d_nu = reinterpret_cast<int64_t*>(ub.get<char>() + (size_t)nu * sizeof(part_unit));
+    GX_CUDA(cudaMemcpyAsync(ub.get(), hu.data(), (size_t)nu * sizeof(part_unit), cudaMemcpyHostToDevice, s));
+    GX_CUDA(cudaMemcpyAsync(d_nu, &nu, 8, cudaMemcpyHostToDevice, s));
+    // No unit is a whole partition, so no final records are appended.
+    uint64_t* no_rec = reinterpret_cast<uint64_t*>(d_nu + 1);
+    unsigned long long* no_cnt = reinterpret_cast<unsigned long long*>(d_nu + 2);
+    int* no_ovf = reinterpret_cast<int*>(d_nu + 3);
+    const bool ok = hash_units_aggregate(key.data, size_of(key.type), vkind_of(key.type), d, ub.get<part_unit>(), d_nu,
+                                         groups, 0, g.recs, g.mask + 1, g.sentinel_flag, no_rec, no_cnt, 0, no_ovf, s,
+                                         true);
+    if (ok) GX_CUDA(cudaStreamSynchronize(s));  // the unit list lives in this scope
+    return ok;
+}
+
 static bool hash_groupby_run(const col& key, int out_key_type, const agg_plan& p, uint64_t cap, int smem_mode,
-                             uint32_t s_slots, int reps, int64_t out_capacity, cudaStream_t s, gx_table* out) {
+                             int64_t units_groups, uint32_t s_slots, int reps, int64_t out_capacity, cudaStream_t s,
+                             gx_table* out) {
     const agg_desc& d = p.d;
     int kw = size_of(key.type);
     uint64_t empty = kw == 4 ? G_EMPTY4 : G_EMPTY8;
@@ -1034,7 +1063,8 @@ static bool hash_groupby_run(const col& key, int out_key_type, const agg_plan& p
     g.sentinel_flag = flags.get<int>();
     g.overflow = flags.get<int>() + 1;
     int kind = vkind_of(key.type);
-    if (key.n > 0) {
+    const bool units = key.n > 0 && units_groups > 0 && hash_groupby_units(key, d, units_groups, g, s);
+    if (key.n > 0 && !units) {
         size_t smem = 0;
         if (smem_mode)
             smem = (((size_t)s_slots * kw + 15) & ~size_t(15)) + (((size_t)s_slots * 4 * reps + 15) & ~size_t(15)) +
@@ -1094,9 +1124,17 @@ void hash_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hint, c
         smem_mode = top >= 0.05f;
     }
     if (const char* e = getenv("GX_HASH_SMEM")) smem_mode = atoi(e) != 0;
+    // A few thousand groups at most: the dense-id unit kernel on row ranges.
+    // (8-byte keys with a few hundred groups or fewer stay on the shared-table
+    // kernel: int64 keys, G = 16: 2.16 ms there against 2.37 through units.)
+    const int64_t units_groups = bound <= HASH_UNITS_MAX_GROUPS && (size_of(key.type) == 4 || bound > 256) &&
+                                         smem_mode && !getenv("GX_HASH_NO_UNITS")
+                                     ? bound
+                                     : 0;
     int64_t out_cap = std::min<int64_t>(n, hint->groups_upper_bound > 0 ? hint->groups_upper_bound : n);
     for (int attempt = 0; attempt < 6; ++attempt) {
-        if (hash_groupby_run(key, key_in.type, p, cap, smem_mode, s_slots, reps, out_cap, s, out)) return;
+        if (hash_groupby_run(key, key_in.type, p, cap, smem_mode, units_groups, s_slots, reps, out_cap, s, out))
+            return;
         cap *= 4;
     }
     fail(GX_EOVERFLOW, "hash group-by table overflow after retries");
@@ -1104,7 +1142,8 @@ void hash_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hint, c
 
 bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d, const part_unit* units,
                           const int64_t* n_units, int64_t gpp, int shift, uint64_t* grec, uint64_t gcap, int* gflags,
-                          uint64_t* orec, unsigned long long* ocount, int64_t rec_cap, int* rec_ovf, cudaStream_t s) {
+                          uint64_t* orec, unsigned long long* ocount, int64_t rec_cap, int* rec_ovf, cudaStream_t s,
+                          bool dense_only) {
     const size_t budget = 200 * 1024;
     const size_t per_rep = 4 + 8 * (size_t)d.n_acc;
     // Slots for the fullest partition expected (Poisson tail), at load <= 1/4:
@@ -1119,14 +1158,17 @@ bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d,
         // keys) for the fullest partition expected, and as many replicas (a
         // power of two, at most 16) as the budget holds.
         const uint32_t ids = (uint32_t)((((uint64_t)std::ceil(gmax)) + 31) & ~uint64_t(31));
-        const size_t fixed = (size_t)slots * 8 + (((size_t)ids * kw + 15) & ~size_t(15));
+        uint32_t dslots = slots;
         auto need = [&](size_t r) {
-            return fixed + (((size_t)ids * r * 4 + 15) & ~size_t(15)) + (size_t)ids * r * 8 * d.n_acc;
+            return (size_t)dslots * 8 + (((size_t)ids * kw + 15) & ~size_t(15)) +
+                   (((size_t)ids * r * 4 + 15) & ~size_t(15)) + (size_t)ids * r * 8 * d.n_acc;
         };
+        // Slots at load <= 1/4, else <= 1/2 (e.g. ~2K groups with 7 aggregates).
+        if (need(1) > budget) dslots = (uint32_t)next_pow2((uint64_t)std::max(64.0, 2.0 * gmax));
         size_t r = 16;
         while (r > 1 && need(r) > budget) r >>= 1;
         if (need(r) <= budget) {
-            const units_args a{keys, kind, units, n_units, slots, (int)r, shift,
+            const units_args a{keys, kind, units, n_units, dslots, (int)r, shift,
                                gtable{grec, gcap - 1, gflags, gflags + 1}, orec, ocount, rec_cap, rec_ovf};
             const uint32_t g32 = (uint32_t)std::min<int64_t>(std::max<int64_t>(gpp, 1), ids);
             if (kw == 4 ? units_dense_dispatch<4>(grid, need(r), s, d, a, ids, g32)
@@ -1136,6 +1178,7 @@ bool hash_units_aggregate(const void* keys, int kw, int kind, const agg_desc& d,
             }
         }
     }
+    if (dense_only) return false;
     // When load 1/4 does not fit (e.g. ~512 groups per partition with 7
     // aggregates), load 1/2 still beats the per-partition fallback kernel
     // by 3x (19.5 -> ~6.5 ms at 2^26.8 rows, 2^17 groups).

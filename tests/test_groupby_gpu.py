@@ -334,6 +334,8 @@ def test_partition_min_max_large_units(monkeypatch, pattern, slot_table, kdt):
     ("GX_HASH_GENERIC", gx.PARTITION, 1 << 16),
     ("GX_PART_OLD_AGG", gx.PARTITION, 1 << 16),  # per-partition CTA aggregation kernel
     ("GX_UNITS_SLOT_TABLE", gx.PARTITION, 1 << 16),  # slot-indexed unit tables instead of dense group ids
+    ("GX_HASH_NO_UNITS", gx.HASH, 1024),  # HASH's shared-table kernel instead of dense-id units on row ranges
+    ("GX_HASH_NO_UNITS", gx.HASH, 2048),
 ])
 def test_forced_alternative_kernels(monkeypatch, env, algo, G):
     # The switches route a plan through its alternative kernel; results must
