@@ -539,10 +539,12 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
 //
 // Insertion claims an empty slot (id PENDING), takes the next id, writes
 // the key of the id and publishes the slot word.  A row that finds its slot
-// PENDING (or, for 8-byte keys, the id's key not yet visible) re-reads a
-// bounded number of times; when the wait, the ids (gcap) or the probe walk
-// run out, the row goes to the global table and the unit is merged there
-// instead of appended.
+// PENDING (or, for 8-byte keys, the id's key not yet visible) retries with
+// its whole warp after the warp regroups, a bounded number of rounds; when
+// the rounds, the ids (gcap) or the probe walk run out, the row goes to the
+// global table and the unit is merged there instead of appended.  The
+// replicas a unit uses are chosen per unit (all for a piece of a split
+// partition, one per 16 rows of a group otherwise).
 // ---------------------------------------------------------------------------
 constexpr unsigned long long UD_EMPTY = ~0ull;
 constexpr uint32_t UD_PENDING = 0xFFFFFFFEu;
