@@ -523,7 +523,8 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_hash_units(const void* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// Unit aggregation with dense group ids (compiled plans).
+// Unit aggregation with dense group ids (compiled plans, or the run-time
+// aggregation list with up to four value columns of any width).
 //
 // k_hash_units indexes its accumulators by table slot, and at the load its
 // tables run at (<= 1/4) the slots leave room for one accumulator replica.
@@ -658,7 +659,7 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const void* __restric
                                                             gtable g, uint64_t* __restrict__ out_recs,
                                                             unsigned long long* __restrict__ out_count,
                                                             int64_t rec_cap, int* __restrict__ rec_ovf) {
-    static_assert(sizeof...(ACCS) > 0, "compiled plans only");
+    constexpr bool CP = sizeof...(ACCS) > 0;  // compiled plan: 8-byte columns, straight-line updates
     using kt = typename dtable<KW>::kt;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_fill, s_spill;
@@ -666,7 +667,7 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const void* __restric
     __shared__ uint32_t s_q[HGB_NT / 32][31 + 32 * HU_UNROLL];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    constexpr int NA = (int)sizeof...(ACCS);
+    const int NA = CP ? (int)sizeof...(ACCS) : d.n_acc;
     const size_t GR = (size_t)gcap * reps;  // words per accumulator (layout for `reps` replicas)
     dtable<KW> t;
     t.slots = reinterpret_cast<unsigned long long*>(smem);
@@ -679,6 +680,19 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const void* __restric
     t.gcap = gcap;
     // tag of a key in its slot word: the key (4 bytes) or its hash (8 bytes)
     auto tag_of = [](uint64_t k, uint32_t h) { return KW == 4 ? (uint32_t)k : h; };
+    // Row i's value lanes, and one row's accumulator updates at word `at` of
+    // the accumulator arrays starting at `ma`.
+    auto load_vals = [&](int64_t i, uint64_t (&vv)[NV]) {
+#pragma unroll
+        for (int c = 0; c < NV; ++c) {
+            if constexpr (CP) vv[c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
+            else vv[c] = c < d.n_cols ? dev_::load_lane(d.col_ptr[c], d.col_width[c], d.col_kind[c], i) : 0ull;
+        }
+    };
+    auto update = [&](uint64_t* ma, uint32_t at, const uint64_t (&vv)[NV]) {
+        if constexpr (CP) spec::apply_all<0, ACCS...>(ma, (uint32_t)GR, at, vv);
+        else dev_::shared_row_update<NV>(ma, GR, (int)at, d, vv);
+    };
     const int64_t nu = *n_units;
     for (int64_t u = blockIdx.x; u < nu; u += gridDim.x) {
         const part_unit un = units[u];
@@ -714,8 +728,7 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const void* __restric
             uint64_t vq[NV];
             if (live) {
                 kq = (kt)ud_load_key<KW>(keys, i, key_kind);
-#pragma unroll
-                for (int c = 0; c < NV; ++c) vq[c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
+                load_vals(i, vq);
             }
             const uint32_t hq = live ? key_hash<KW>(kq) : 0u;
             const uint32_t gq = d_find_or_insert_warp<KW>(t, live, kq, tag_of(kq, hq), hq >> shift);
@@ -723,7 +736,7 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const void* __restric
             if (!live) return;
             if (gq < gcap) {
                 atomicAdd(&my_counts[gq * R], 1u);
-                spec::apply_all<0, ACCS...>(my_acc, (uint32_t)GR, gq * R, vq);
+                update(my_acc, gq * R, vq);
             } else {
                 if (!s_spill) s_spill = 1;
                 uint64_t* r = g_find_or_insert<KW>(g, d, kq, hq);
@@ -739,9 +752,7 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const void* __restric
                 const int64_t i = base + q * HGB_NT + threadIdx.x;
                 if (i < un.end) {
                     kw[q] = (kt)ud_load_key<KW>(keys, i, key_kind);
-#pragma unroll
-                    for (int c = 0; c < NV; ++c)
-                        v[q][c] = __ldg(static_cast<const unsigned long long*>(d.col_ptr[c]) + i);
+                    load_vals(i, v[q]);
                 }
             }
             // First probe of every row at once; a row whose home slot holds
@@ -772,7 +783,7 @@ __global__ void __launch_bounds__(HGB_NT, 1) k_units_dense(const void* __restric
                 qfill += __popc(mm);
                 if (hit) {
                     atomicAdd(&my_counts[gid[q] * R], 1u);
-                    spec::apply_all<0, ACCS...>(my_acc, (uint32_t)GR, gid[q] * R, v[q]);
+                    update(my_acc, gid[q] * R, v[q]);
                 }
             }
             __syncwarp();
@@ -975,9 +986,8 @@ static bool try_units_spec(int grid, size_t smem, cudaStream_t s, const agg_desc
 }
 
 template <int KW, int NV, class... ACCS>
-static bool try_units_dense(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a,
-                            uint32_t gcap, uint32_t gpp) {
-    if (d.n_cols != NV || !plan_matches<ACCS...>(d)) return false;
+static bool launch_units_dense(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a,
+                               uint32_t gcap, uint32_t gpp) {
     GX_PROF("partition_aggregate", s);
     GX_CUDA(cudaFuncSetAttribute(k_units_dense<KW, NV, ACCS...>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
@@ -986,20 +996,33 @@ static bool try_units_dense(int grid, size_t smem, cudaStream_t s, const agg_des
                                                               a.rec_cap, a.rec_ovf);
     return true;
 }
-// The dense-id kernel for a compiled plan; false when the plan has no
-// compiled form.
+
+template <int KW, int NV, class... ACCS>
+static bool try_units_dense(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a,
+                            uint32_t gcap, uint32_t gpp) {
+    if (d.n_cols != NV || !plan_matches<ACCS...>(d)) return false;
+    return launch_units_dense<KW, NV, ACCS...>(grid, smem, s, d, a, gcap, gpp);
+}
+
+// The dense-id kernel: a compiled plan when one matches (GX_HASH_GENERIC
+// skips them), else the run-time aggregation list; false for more than four
+// value columns.
 template <int KW>
 static bool units_dense_dispatch(int grid, size_t smem, cudaStream_t s, const agg_desc& d, const units_args& a,
                                  uint32_t gcap, uint32_t gpp) {
     using namespace spec;
-    if (getenv("GX_HASH_GENERIC")) return false;
-    if (try_units_dense<KW, 1, A<OP_SUM, VK_I, 0>>(grid, smem, s, d, a, gcap, gpp)) return true;
-    if (try_units_dense<KW, 1, A<OP_SUM, VK_F, 0>>(grid, smem, s, d, a, gcap, gpp)) return true;
-    if (try_units_dense<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_MIN, VK_I, 0>, A<OP_MAX, VK_I, 0>, A<OP_SUM, VK_F, 1>,
-                        A<OP_MIN, VK_F, 1>, A<OP_MAX, VK_F, 1>>(grid, smem, s, d, a, gcap, gpp))
-        return true;
-    if (try_units_dense<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_SUM, VK_I, 1>>(grid, smem, s, d, a, gcap, gpp)) return true;
-    return false;
+    if (!getenv("GX_HASH_GENERIC")) {
+        if (try_units_dense<KW, 1, A<OP_SUM, VK_I, 0>>(grid, smem, s, d, a, gcap, gpp)) return true;
+        if (try_units_dense<KW, 1, A<OP_SUM, VK_F, 0>>(grid, smem, s, d, a, gcap, gpp)) return true;
+        if (try_units_dense<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_MIN, VK_I, 0>, A<OP_MAX, VK_I, 0>, A<OP_SUM, VK_F, 1>,
+                            A<OP_MIN, VK_F, 1>, A<OP_MAX, VK_F, 1>>(grid, smem, s, d, a, gcap, gpp))
+            return true;
+        if (try_units_dense<KW, 2, A<OP_SUM, VK_I, 0>, A<OP_SUM, VK_I, 1>>(grid, smem, s, d, a, gcap, gpp)) return true;
+    }
+    if (d.n_cols > 4) return false;
+    if (d.n_cols <= 1) return launch_units_dense<KW, 1>(grid, smem, s, d, a, gcap, gpp);
+    if (d.n_cols <= 2) return launch_units_dense<KW, 2>(grid, smem, s, d, a, gcap, gpp);
+    return launch_units_dense<KW, 4>(grid, smem, s, d, a, gcap, gpp);
 }
 
 template <int KW>

@@ -287,7 +287,9 @@ struct pb_layout {
     uint32_t whist, qsum, pk, gbase, dbase, total;
 };
 
-__host__ __device__ inline pb_layout pb_make_layout(const move_cols& mc) {
+// Shared-memory layout; the per-warp counts of the stable ranking are only
+// laid out when `stable`.
+__host__ __device__ inline pb_layout pb_make_layout(const move_cols& mc, bool stable) {
     pb_layout L{};
     uint32_t o = 0;
     for (int c = 0; c < mc.n; ++c) {
@@ -296,8 +298,8 @@ __host__ __device__ inline pb_layout pb_make_layout(const move_cols& mc) {
     }
     L.stage_bytes = o;
     o *= 2;
-    L.whist = o; o += PB_WARPS * PS_BINS * 2;   // u16 per-warp digit counts
-    L.qsum = o;  o += 4 * PS_BINS * 2;          // u16 sums over 8-warp quarters
+    L.whist = o; if (stable) o += PB_WARPS * PS_BINS * 2;   // u16 per-warp digit counts
+    L.qsum = o;  if (stable) o += 4 * PS_BINS * 2;          // u16 sums over 8-warp quarters
     L.pk = o;    o += PS_TILE * 4;              // u32 per staged position: source row | digit << 16
     L.gbase = o; o += PS_BINS * 8;              // int64 output base per digit
     L.dbase = o; o += PS_BINS * 4;              // u32 first staged position per digit
@@ -793,10 +795,11 @@ void partition_starts(const void* keys, int kw, int64_t n, int kind, int R, int6
 
 namespace {
 
-// The bulk-copy scatter applies when every loaded column is 4 or 8 bytes
-// wide and 16-byte aligned, and two tiles of them fit in shared memory.
+// The bulk-copy scatter applies to 2..4 moved columns when every loaded
+// column is 4 or 8 bytes wide and 16-byte aligned, and two tiles of them fit
+// in shared memory (four columns: up to 24 B per row, single-pass ranking).
 static bool bulk_scatter_ok(const move_cols& mc, const pb_layout& L) {
-    if (getenv("GX_PART_NO_BULK") || mc.n < 2 || mc.n > 3) return false;
+    if (getenv("GX_PART_NO_BULK") || mc.n < 2 || mc.n > 4) return false;
     for (int c = 0; c < mc.n; ++c) {
         if (mc.iota[c]) continue;
         if (mc.width[c] != 4 && mc.width[c] != 8) return false;
@@ -813,7 +816,7 @@ void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_
     k_part_hist<KW><<<hist_grid, PH_NT, 0, s>>>(kin, n, kind, shift, dbits, ntiles, counts);
     GX_LAUNCHED();
     exclusive_scan_i64(counts, offs, ((int64_t)1 << dbits) * ntiles, s);
-    const pb_layout L = pb_make_layout(mc);
+    const pb_layout L = pb_make_layout(mc, stable);
     if (bulk_scatter_ok(mc, L)) {
         static per_device_flag battr;
         battr.once([] {
@@ -822,6 +825,8 @@ void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_
             GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
         });
         const int grid = (int)std::min<int64_t>(ntiles, dev().sm_count);
         GX_PROF("partition_scatter", s);
@@ -829,8 +834,10 @@ void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_
     k_part_scatter_bulk<KW, NCV, ST><<<grid, PB_NT, L.total, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc, L, err)
         if (mc.n == 2 && stable) GX_PB_LAUNCH(2, true);
         else if (mc.n == 2) GX_PB_LAUNCH(2, false);
-        else if (stable) GX_PB_LAUNCH(3, true);
-        else GX_PB_LAUNCH(3, false);
+        else if (mc.n == 3 && stable) GX_PB_LAUNCH(3, true);
+        else if (mc.n == 3) GX_PB_LAUNCH(3, false);
+        else if (stable) GX_PB_LAUNCH(4, true);
+        else GX_PB_LAUNCH(4, false);
 #undef GX_PB_LAUNCH
         GX_LAUNCHED();
         return;

@@ -332,6 +332,8 @@ def test_partition_min_max_large_units(monkeypatch, pattern, slot_table, kdt):
 @pytest.mark.parametrize("env,algo,G", [
     ("GX_HASH_GENERIC", gx.HASH, 4096),      # run-time aggregation list instead of a compiled plan
     ("GX_HASH_GENERIC", gx.PARTITION, 1 << 16),
+    ("GX_HASH_GENERIC+GX_UNITS_SLOT_TABLE", gx.PARTITION, 1 << 16),  # run-time list, slot-indexed unit tables
+    ("GX_HASH_GENERIC+GX_HASH_NO_UNITS", gx.HASH, 1024),  # run-time list, HASH's shared-table kernel
     ("GX_PART_OLD_AGG", gx.PARTITION, 1 << 16),  # per-partition CTA aggregation kernel
     ("GX_UNITS_SLOT_TABLE", gx.PARTITION, 1 << 16),  # slot-indexed unit tables instead of dense group ids
     ("GX_HASH_NO_UNITS", gx.HASH, 1024),  # HASH's shared-table kernel instead of dense-id units on row ranges
@@ -345,8 +347,43 @@ def test_forced_alternative_kernels(monkeypatch, env, algo, G):
     iv = O.gen_values(n, np.int64, lo=-(1 << 35), hi=1 << 35, seed=52)
     fv = O.gen_values(n, np.float64, seed=53)
     reqs = [(0, gx.SUM), (0, gx.MIN), (0, gx.MAX), (1, gx.SUM), (1, gx.MIN), (1, gx.MAX), (0, gx.COUNT_ALL)]
-    monkeypatch.setenv(env, "1")
+    for e in env.split("+"):
+        monkeypatch.setenv(e, "1")
     got, exp, _ = run_both(key, [iv, fv], reqs, algo, bound=G)
+    assert_columns_match(got, exp)
+
+
+@pytest.mark.parametrize("ncols", [3, 5])
+@pytest.mark.parametrize("algo,G", [(gx.HASH, 1024), (gx.PARTITION, 1 << 16), (gx.AUTO_ALGO, 1 << 16)])
+def test_many_value_columns(algo, G, ncols):
+    # Run-time aggregation lists over three or five value columns of mixed
+    # widths: the dense-id unit kernel takes up to four columns, the
+    # slot-indexed one (or HASH's shared-table kernel) more, and PARTITION
+    # moves more than three columns through the register-staged scatter.
+    n = (1 << 19) + 77
+    key = O.gen_keys(n, np.int32, groups=G, scatter=1, seed=61)
+    cols = [O.gen_values(n, np.int64, lo=-(1 << 40), hi=1 << 40, seed=62),
+            O.gen_values(n, np.float64, seed=63),
+            O.gen_values(n, np.int32, lo=-(1 << 20), hi=1 << 20, seed=64),
+            O.gen_values(n, np.float32, seed=65),
+            O.gen_values(n, np.int16, lo=-1000, hi=1000, seed=66)][:ncols]
+    reqs = [(0, gx.SUM), (1, gx.SUM), (2, gx.MIN), (2, gx.MAX), (0, gx.COUNT_ALL)]
+    if ncols == 5:
+        reqs += [(3, gx.MAX), (4, gx.SUM), (4, gx.MIN)]
+    got, exp, _ = run_both(key, cols, reqs, algo, bound=G)
+    assert_columns_match(got, exp)
+
+
+@pytest.mark.parametrize("bits", [8, 12])
+def test_partition_four_moved_columns(bits):
+    # Key + three 4-byte value columns (16 B per row): the bulk-copy scatter
+    # with four moved columns, over 12 radix bits in two passes (the second
+    # with the stable ranking).
+    n = (1 << 19) + 77
+    key = O.gen_keys(n, np.int32, groups=1 << 16, scatter=1, seed=81)
+    cols = [O.gen_values(n, np.int32, lo=-(1 << 30), hi=1 << 30, seed=82 + i) for i in range(3)]
+    reqs = [(0, gx.SUM), (1, gx.MIN), (2, gx.MAX), (0, gx.COUNT_ALL)]
+    got, exp, _ = run_both(key, cols, reqs, gx.PARTITION, bound=1 << 16, radix_bits=bits)
     assert_columns_match(got, exp)
 
 
