@@ -172,6 +172,7 @@ def _load() -> C.CDLL:
         "gx_selector_plan_features": ([tv, C.POINTER(AggRequest), i32, i32, vp], i32),
         "gx_selector_param_count": ([], i64),
         "gx_selector_load": ([vp, vp, vp], i32),
+        "gx_selector_set_plan_support": ([vp, i32, C.c_float], i32),
         "gx_selector_predict": ([vp, i32, vp], i32),
         "gx_mlp_forward": ([vp, vp, i32, vp, vp], i32),
         "gx_mlp_forward_backward": ([vp, vp, vp, vp, i32, vp, vp, vp], i32),
@@ -612,8 +613,10 @@ def gather(gather_map, col, stream=None):
 
 
 def compute_ndv_approx(col, stream=None) -> int:
+    """HyperLogLog distinct-count estimate of a device column (a tensor or a
+    ColumnView)."""
     nd = C.c_int64()
-    check(lib.gx_compute_ndv_approx(view(col), _stream_ptr(stream), C.byref(nd)))
+    check(lib.gx_compute_ndv_approx(_column_view(col), _stream_ptr(stream), C.byref(nd)))
     return int(nd.value)
 
 

@@ -37,6 +37,7 @@ void selector_features(const col& key, float* f, cudaStream_t s);
 void selector_plan_features(const agg_plan& p, float* f4);
 int64_t selector_param_count();
 void selector_load(const uint16_t* params, const float* mean, const float* stdv);
+void selector_set_plan_support(const float* f4, int count, float radius);
 void selector_predict(const float* feats, int rows, float* scores, cudaStream_t s);
 void mlp_forward(const void* params, const float* x, int rows, float* out, cudaStream_t s);
 void mlp_forward_backward(const void* params, const float* x, const float* tgt, const float* mask, int rows,
@@ -493,6 +494,13 @@ gx_status gx_selector_load(const uint16_t* params, const float* mean, const floa
     GX_TRY({
         gx::require(params != nullptr, "null weights");
         gx::selector_load(params, mean, stdv);
+    })
+}
+gx_status gx_selector_set_plan_support(const float* plan_features, int32_t count, float radius) {
+    GX_TRY({
+        gx::require(count >= 0 && (count == 0 || plan_features != nullptr), "bad plan support list");
+        gx::require(radius >= 0.f, "negative support radius");
+        gx::selector_set_plan_support(plan_features, count, radius);
     })
 }
 gx_status gx_selector_predict(const float* features, int32_t rows, float* scores) {

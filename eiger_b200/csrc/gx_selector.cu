@@ -150,6 +150,10 @@ struct selector_state {
     std::vector<uint16_t> params;
     float mean[F], stdv[F];
     void* dparams[16] = {};
+    // Plan features (16..19) of the request lists the weights were trained
+    // on, and how far from them the network is trusted; empty: everywhere.
+    std::vector<float> support;
+    float radius = 0.f;
 };
 selector_state g_sel;
 
@@ -264,6 +268,26 @@ bool selector_loaded() {
     return g_sel.loaded;
 }
 
+void selector_set_plan_support(const float* f4, int count, float radius) {
+    std::lock_guard<std::mutex> g(g_sel.mu);
+    g_sel.support.assign(f4, f4 + (size_t)count * (F - GX_SEL_KEY_FEATURES));
+    g_sel.radius = radius;
+}
+
+// Whether the network has seen a request list like this one: plan features
+// within the radius (largest coordinate difference) of a registered one.
+static bool plan_in_support(const float* f4) {
+    constexpr int PF = F - GX_SEL_KEY_FEATURES;
+    std::lock_guard<std::mutex> g(g_sel.mu);
+    if (g_sel.support.empty()) return true;
+    for (size_t b = 0; b < g_sel.support.size(); b += PF) {
+        float d = 0.f;
+        for (int i = 0; i < PF; ++i) d = std::max(d, std::fabs(f4[i] - g_sel.support[b + i]));
+        if (d <= g_sel.radius) return true;
+    }
+    return false;
+}
+
 static const __half* selector_device_params() {
     int d = dev().device;
     std::lock_guard<std::mutex> g(g_sel.mu);
@@ -317,16 +341,21 @@ void selector_predict(const float* feats, int rows, float* scores, cudaStream_t 
 }
 
 // AUTO with the learned selector; falls back to the reference's NDV rule
-// when no weights are loaded.
+// when no weights are loaded or the request list is outside the support
+// registered with the weights.
 int selector_choose(const col& key, const agg_plan& plan, int* radix_bits, cudaStream_t s) {
     *radix_bits = 0;
-    if (!selector_loaded()) {
+    float pf[F - GX_SEL_KEY_FEATURES];
+    selector_plan_features(plan, pf);
+    // No weights, or a request list unlike those the weights were trained
+    // on (the network's scores there are extrapolations): the plain rule.
+    if (!selector_loaded() || !plan_in_support(pf)) {
         int64_t est = ndv_estimate(key, s);
         return est <= (size_of(key.type) == 4 ? (1 << 14) : (1 << 18)) ? GX_GB_HASH : GX_GB_PARTITION;
     }
     float f[F], y[O];
     selector_features(key, f, s);
-    selector_plan_features(plan, f + GX_SEL_KEY_FEATURES);
+    std::copy(pf, pf + (F - GX_SEL_KEY_FEATURES), f + GX_SEL_KEY_FEATURES);
     selector_predict(f, 1, y, s);
     static const int variants[3] = {GX_GB_HASH, GX_GB_SORT, GX_GB_PARTITION};
     int best = 0;

@@ -273,8 +273,29 @@ def save(path: Path, params_u16: np.ndarray, mean: np.ndarray, std: np.ndarray, 
              meta=json.dumps(meta), version=1)
 
 
+# How far (largest difference of one plan feature) a request list may lie
+# from a trained one for AUTO to trust the network: SUM + COUNT over an int32
+# column (0.125 from the int64 training list) stays inside; SUM over a
+# float64 column, or an extra accumulator class, does not.
+SUPPORT_RADIUS = 0.13
+
+
+def training_plan_support() -> np.ndarray:
+    """Plan features (16..19) of the request lists in AGGS, over the value
+    columns make_instance builds (int64, then float64), computed by the
+    library on the host: one row per list."""
+    gx = _gx()
+    cols = [gx.ColumnView(None, 0, gx.INT64, 0), gx.ColumnView(None, 0, gx.FLOAT64, 0)]
+    rows = []
+    for reqs in AGGS.values():
+        ncols = max(c for c, _ in reqs) + 1
+        rows.append(plan_features(cols[:ncols], reqs))
+    return np.ascontiguousarray(np.stack(rows), np.float32)
+
+
 def install(path: Path | None = None) -> bool:
-    """Load trained weights into the library (AUTO + hint.selector=LEARNED)."""
+    """Load trained weights into the library (AUTO + hint.selector=LEARNED),
+    with the request lists they were trained on as the network's support."""
     gx = _gx()
     path = Path(path) if path else WEIGHTS
     if not path.exists():
@@ -286,6 +307,8 @@ def install(path: Path | None = None) -> bool:
     mean = np.ascontiguousarray(d["mean"], np.float32)
     std = np.ascontiguousarray(d["std"], np.float32)
     gx.check(gx.lib.gx_selector_load(p.ctypes.data, mean.ctypes.data, std.ctypes.data))
+    sup = training_plan_support()
+    gx.check(gx.lib.gx_selector_set_plan_support(sup.ctypes.data, len(sup), SUPPORT_RADIUS))
     return True
 
 

@@ -529,6 +529,13 @@ int64_t gx_selector_param_count(void);
 /* Install trained fp16 weights (host array of gx_selector_param_count halves). */
 gx_status gx_selector_load(const uint16_t* params_fp16_host, const float* feat_mean,
                            const float* feat_std);
+/* The request lists the loaded weights were trained on, as their plan
+ * features (gx_selector_plan_features: 4 floats each, `count` lists): AUTO
+ * with the learned selector runs the network only for a request list whose
+ * plan features lie within `radius` (largest coordinate difference) of one
+ * of them, and the plain NDV rule otherwise.  count = 0 (the state before
+ * any call) trusts the network for every list.  Host only. */
+gx_status gx_selector_set_plan_support(const float* plan_features_host, int32_t count, float radius);
 /* Forward pass for a batch of feature rows on the device: writes
  * GX_SEL_NUM_OUTPUTS scores per row (lower is better). */
 gx_status gx_selector_predict(const float* features_host, int32_t rows, float* scores_host);

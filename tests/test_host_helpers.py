@@ -67,3 +67,23 @@ def test_string_dictionary_is_distinct_ascii_with_arrow_offsets():
     assert len(words) == 2000
     c2, o2 = batch.make_dictionary(2000, seed=3, min_len=8, max_len=32)
     assert np.array_equal(chars, c2) and np.array_equal(offs, o2)
+
+
+def test_selector_support_holds_the_training_lists():
+    # The plan features AUTO compares a request list with before it trusts
+    # the network (host only): the two training lists, a near neighbour
+    # inside the radius and a list with another accumulator mix outside it.
+    import eiger_b200 as gx
+    sup = selector.training_plan_support()
+    assert np.allclose(sup, [[0.25, 0.125, 0.0, 0.0], [0.5, 0.75, 0.25, 0.5]])
+    i32 = [gx.ColumnView(None, 0, gx.INT32, 0)]
+    near = selector.plan_features(i32, [(0, gx.SUM), (0, gx.COUNT_ALL)])
+    two = [gx.ColumnView(None, 0, gx.INT64, 0), gx.ColumnView(None, 0, gx.FLOAT64, 0)]
+    far = selector.plan_features(two, [(1, gx.SUM), (0, gx.MAX), (0, gx.COUNT_ALL)])
+
+    def dist(f):
+        return float(np.abs(sup - f).max(axis=1).min())
+
+    assert dist(near) <= selector.SUPPORT_RADIUS < dist(far)
+    assert gx.lib.gx_selector_set_plan_support(None, -1, 0.1) != 0
+    assert gx.lib.gx_selector_set_plan_support(sup.ctypes.data, len(sup), -1.0) != 0

@@ -112,3 +112,23 @@ def test_auto_with_learned_selector_is_exact():
         assert hint.groupby_algo in (gx.HASH, gx.SORT, gx.PARTITION)
         exp = O.groupby(key, [val], [(0, O.SUM), (0, O.COUNT_ALL)])
         assert_columns_match(sort_by_key(t.numpy_columns()), exp)
+
+
+def test_auto_outside_the_trained_request_lists_uses_the_plain_rule():
+    # A request list unlike the two the weights were trained on (here SUM f64
+    # + MAX i64 + COUNT): AUTO does not extrapolate the network but takes the
+    # plain NDV rule (<= 2^14 distinct 4-byte keys -> HASH, else PARTITION).
+    from eiger_b200 import selector as S
+    if not S.install():
+        pytest.skip("no trained selector weights committed")
+    n = 1 << 18
+    iv = O.gen_values(n, np.int64, lo=0, hi=1 << 31, seed=71)
+    fv = O.gen_values(n, np.float64, seed=72)
+    reqs = [(1, gx.SUM), (0, gx.MAX), (0, gx.COUNT_ALL)]
+    for G, want in ((1000, gx.HASH), (1 << 17, gx.PARTITION)):
+        key = O.gen_keys(n, np.int32, groups=G, scatter=1, seed=73)
+        hint = gx.make_hint(gx.AUTO_ALGO, selector=gx.SELECT_LEARNED)
+        t = gx.groupby([to_dev(key)], [to_dev(iv), to_dev(fv)], reqs, hint)
+        assert hint.groupby_algo == want
+        exp = O.groupby(key, [iv, fv], [(1, O.SUM), (0, O.MAX), (0, O.COUNT_ALL)])
+        assert_columns_match(sort_by_key(t.numpy_columns()), exp)
