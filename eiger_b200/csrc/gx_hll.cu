@@ -54,6 +54,55 @@ __global__ void k_hll(const void* __restrict__ keys, int64_t n, int64_t stride, 
         if (sreg[i]) atomicMax(&regs[i], sreg[i]);
 }
 
+// Full-column sketch of a 16-byte aligned key column: 16-byte loads, four
+// in flight per thread (the strided kernel above keeps one 4-byte load in
+// flight per thread, too few to cover HBM latency); the n % (16 / KW) tail
+// keys are added by block 0.  Same registers as k_hll (max is order-free).
+constexpr int HLLV_NT = 512, HLLV_VEC = 4;
+template <int KW>
+__global__ void __launch_bounds__(HLLV_NT) k_hll_vec(const void* __restrict__ keys, int64_t n, int kind,
+                                                     unsigned* __restrict__ regs) {
+    __shared__ unsigned sreg[HLL_M];
+    for (int i = threadIdx.x; i < HLL_M; i += HLLV_NT) sreg[i] = 0;
+    __syncthreads();
+    auto add = [&](uint64_t b) {
+        uint32_t idx, rank;
+        hll_index_rank(hll_hash(b), &idx, &rank);
+        if (sreg[idx] < rank) atomicMax(&sreg[idx], rank);
+    };
+    constexpr int KPV = 16 / KW;  // keys per 16-byte vector
+    const int64_t nvec = n / KPV;
+    const uint4* kv = static_cast<const uint4*>(keys);
+    const int64_t step = (int64_t)gridDim.x * HLLV_NT;
+    for (int64_t v0 = blockIdx.x * (int64_t)HLLV_NT + threadIdx.x; v0 < nvec; v0 += step * HLLV_VEC) {
+        uint4 x[HLLV_VEC] = {};
+#pragma unroll
+        for (int q = 0; q < HLLV_VEC; ++q)
+            if (v0 + q * step < nvec) x[q] = __ldcs(kv + v0 + q * step);
+#pragma unroll
+        for (int q = 0; q < HLLV_VEC; ++q) {
+            if (v0 + q * step >= nvec) break;
+            if (KW == 4) {
+                add(canon32(x[q].x, kind));
+                add(canon32(x[q].y, kind));
+                add(canon32(x[q].z, kind));
+                add(canon32(x[q].w, kind));
+            } else {
+                add(canon64(((uint64_t)x[q].y << 32) | x[q].x, kind));
+                add(canon64(((uint64_t)x[q].w << 32) | x[q].z, kind));
+            }
+        }
+    }
+    if (blockIdx.x == 0)
+        for (int64_t i = nvec * KPV + threadIdx.x; i < n; i += HLLV_NT) {
+            if (KW == 4) add(canon32(__ldg(static_cast<const unsigned*>(keys) + i), kind));
+            else add(canon64(__ldg(static_cast<const unsigned long long*>(keys) + i), kind));
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < HLL_M; i += HLLV_NT)
+        if (sreg[i]) atomicMax(&regs[i], sreg[i]);
+}
+
 template <int KW>
 __global__ void k_minmax(const void* __restrict__ keys, int64_t n, int kind, unsigned long long* out) {
     // Track the order-preserving image; convert back on the host.
@@ -104,8 +153,18 @@ void hll_registers(const col& key_in, int64_t n, int64_t stride, unsigned* d_reg
     GX_CUDA(cudaMemsetAsync(d_regs, 0, HLL_M * sizeof(unsigned), s));
     if (n <= 0) return;
     int kind = vkind_of(key.type);
+    const int kw = size_of(key.type);
+    if (stride == 1 && reinterpret_cast<uintptr_t>(key.data) % 16 == 0 && n >= (int64_t)HLLV_NT * 16) {
+        // Two CTAs per SM; fewer for small columns (each CTA merges 2^13
+        // registers into the global sketch).
+        const int g = (int)std::min<int64_t>((int64_t)dev().sm_count * 2, ceil_div(n, (int64_t)HLLV_NT * 64));
+        if (kw == 4) k_hll_vec<4><<<g, HLLV_NT, 0, s>>>(key.data, n, kind, d_regs);
+        else k_hll_vec<8><<<g, HLLV_NT, 0, s>>>(key.data, n, kind, d_regs);
+        GX_LAUNCHED();
+        return;
+    }
     int g = grid_for(n, 256, 2);
-    if (size_of(key.type) == 4) k_hll<4><<<g, 256, 0, s>>>(key.data, n, stride, kind, d_regs);
+    if (kw == 4) k_hll<4><<<g, 256, 0, s>>>(key.data, n, stride, kind, d_regs);
     else k_hll<8><<<g, 256, 0, s>>>(key.data, n, stride, kind, d_regs);
     GX_LAUNCHED();
 }

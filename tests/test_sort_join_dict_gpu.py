@@ -248,12 +248,28 @@ def test_dictionary_encode_with_dict():
 
 # ------------------------------------------------------------ hll / gen ----
 @pytest.mark.parametrize("kdt,G", [(np.int32, 1000), (np.int64, 1 << 18), (np.int32, 1 << 22)])
-def test_hll_matches_oracle_registers(kdt, G):
-    k = O.gen_keys(1 << 22, kdt, groups=G, scatter=1, seed=8)
+@pytest.mark.parametrize("extra", [0, 3])
+def test_hll_matches_oracle_registers(kdt, G, extra):
+    # extra = 3: a tail of keys past the last 16-byte vector.
+    k = O.gen_keys((1 << 22) + extra, kdt, groups=G, scatter=1, seed=8)
     est = gx.compute_ndv_approx(to_dev(k))
     exp = O.hll_estimate(O.hll_registers(k))
     assert est == int(round(exp))
     assert abs(est - O.ndv_exact(k)) / O.ndv_exact(k) < 0.04
+
+
+def test_hll_unaligned_view_and_narrow_keys():
+    # A view starting one row into its buffer (not 16-byte aligned: the
+    # strided kernel) and 16-bit keys (widened first): same registers as the
+    # oracle.
+    import torch
+    k = O.gen_keys((1 << 20) + 1, np.int32, groups=5000, scatter=1, seed=9)
+    d = to_dev(k)
+    v = gx.ColumnView(d.data_ptr(), len(k) - 1, gx.INT32, 1)
+    assert (d.data_ptr() + 4) % 16 != 0
+    assert gx.compute_ndv_approx(v) == int(round(O.hll_estimate(O.hll_registers(k[1:]))))
+    k16 = (k % 30000).astype(np.int16)
+    assert gx.compute_ndv_approx(torch.from_numpy(k16).cuda()) == int(round(O.hll_estimate(O.hll_registers(k16))))
 
 
 @pytest.mark.parametrize("dist,kdt", [(O.DIST_UNIFORM, np.int32), (O.DIST_CYCLIC, np.int64),
