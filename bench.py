@@ -369,9 +369,11 @@ def run_gx(args) -> None:
     # ------------------------------------------------------- sweep grid
     # The group-by sweep at the timed row count, every variant: G over the
     # sweep's range (int32 keys, uniform), plus Zipf 1.5 and int64 keys.
-    sweep = None
+    sweep = shapes = operators = None
     if not args.no_sweep:
         sweep = sweep_grid(gx, torch, rows, peaks, dist)
+        shapes = shapes_grid(gx, torch, rows, peaks, sel, dist)
+        operators = operators_grid(gx, torch, rows, peaks, dist)
 
     # ----------------------------------------------------------- batched
     batched = None
@@ -421,7 +423,8 @@ def run_gx(args) -> None:
                        "selector": "learned" if learned else ("plain" if args.algo == "auto" else "forced"),
                        "l2": "inputs (5.4 GB) larger than L2; no flush"},
             "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk.summary(), "join": join, "batched": batched, "sweep": sweep,
+            "clocks": clk.summary(), "join": join, "batched": batched, "sweep": sweep, "shapes": shapes,
+            "operators": operators,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -464,6 +467,89 @@ def sweep_grid(gx, torch, rows: int, peaks: dict, dist=None) -> list:
                         "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)})
         del k, iv, fv, cdf
         torch.cuda.empty_cache()
+    return out
+
+
+def shapes_grid(gx, torch, rows: int, peaks: dict, sel: int, dist=None) -> list:
+    """Group-by requests outside the compiled aggregation plans, through
+    AUTO at `rows` rows: a run-time aggregation list over the int64 + float64
+    columns (2^16 and 2^10 groups), and three value columns (int64, float64,
+    int32), whose rows of four moved columns take the register-staged
+    partition scatter.  Per shape: AUTO's pick with its ms, Grows/s and
+    fraction of measured HBM (algorithmic bytes: every input column read
+    once plus the output records), and the ms of HASH and PARTITION forced."""
+    names = {gx.HASH: "hash", gx.SORT: "sort", gx.SORT_OPT: "sort_opt", gx.SORT_GFUR: "sort_gfur",
+             gx.PARTITION: "partition", gx.PARTITION_GFUR: "partition_gfur"}
+    iv = torch.empty(rows, dtype=torch.int64, device="cuda")
+    gx.generate_values(iv, gx.gen_spec(seed=5, stream_id=1, lo=0, hi=1 << 31))
+    fv = torch.empty(rows, dtype=torch.float64, device="cuda")
+    gx.generate_values(fv, gx.gen_spec(seed=5, stream_id=2))
+    i32 = torch.empty(rows, dtype=torch.int32, device="cuda")
+    gx.generate_values(i32, gx.gen_spec(seed=5, stream_id=3, lo=-(1 << 20), hi=1 << 20))
+    generic = [(1, gx.SUM), (0, gx.MAX), (0, gx.COUNT_ALL)]
+    three = [(0, gx.SUM), (1, gx.SUM), (2, gx.MIN), (2, gx.MAX), (0, gx.COUNT_ALL)]
+    shapes = [("sum f64, max i64, count", 1 << 16, [iv, fv], generic, 2),
+              ("sum f64, max i64, count", 1 << 10, [iv, fv], generic, 2),
+              ("sum i64, sum f64, min/max i32, count (3 value columns)", 1 << 16, [iv, fv, i32], three, 4)]
+    out = []
+    for desc, G, cols, reqs, n_out in shapes:
+        k = torch.empty(rows, dtype=torch.int32, device="cuda")
+        gx.generate_keys(k, gx.gen_spec(seed=5, groups=G, scatter=1))
+        chosen = {}
+
+        def step():
+            h = gx.make_hint(gx.AUTO_ALGO, G, selector=sel)
+            t = gx.groupby([k], cols, reqs, h)
+            chosen["algo"] = h.groupby_algo
+            return t
+
+        r = step()
+        ng = r.num_rows
+        del r
+        ms = time_steps(torch, step, 3, 2, dist) / 3
+        alg = rows * (4 + sum(c.element_size() for c in cols)) + ng * (4 + 8 * n_out)
+        forced = {}
+        for name, algo in (("hash", gx.HASH), ("partition", gx.PARTITION)):
+            forced[name + "_ms"] = round(time_steps(
+                torch, lambda: gx.groupby([k], cols, reqs, gx.make_hint(algo, G)), 3, 2, dist) / 3, 3)
+        out.append({"aggregates": desc, "groups": G, "groups_found": ng, "algo": names.get(chosen["algo"], "?"),
+                    "ms": round(ms, 3), "grows_s": round(rows / ms / 1e6, 2),
+                    "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4), **forced})
+        del k
+    del iv, fv, i32
+    torch.cuda.empty_cache()
+    return out
+
+
+def operators_grid(gx, torch, rows: int, peaks: dict, dist=None) -> list:
+    """The operators beside the group-by, each on its own at `rows` rows
+    (int32 keys uniform over 2^16 scattered values, int64 values in
+    [0, 2^31)): radix sort and 8-bit radix partition of (key, value) pairs,
+    dictionary encode, the HyperLogLog distinct estimate, and a BETWEEN
+    filter keeping half the rows with the compaction of both columns.  Per
+    operator: ms, Grows/s and the fraction of measured HBM for its
+    algorithmic bytes (inputs read once, outputs written once; a 4-pass sort
+    moves about four times that)."""
+    k = torch.empty(rows, dtype=torch.int32, device="cuda")
+    gx.generate_keys(k, gx.gen_spec(seed=11, groups=1 << 16, scatter=1))
+    v = torch.empty(rows, dtype=torch.int64, device="cuda")
+    gx.generate_values(v, gx.gen_spec(seed=11, stream_id=1, lo=0, hi=1 << 31))
+    pair = rows * (4 + 8)
+    half = [gx.predicate(1, gx.CMP_BETWEEN, 0, 1 << 30)]
+    ops = [("radix sort, 32 key bits (int32 key, int64 value)", lambda: gx.sort_column_pair(k, v), 2 * pair),
+           ("radix partition, 8 bits (int32 key, int64 value)", lambda: gx.partition_column_pair(k, v, 0, 8),
+            2 * pair),
+           ("dictionary encode (int32 keys -> int32 codes)", lambda: gx.dictionary_encode(k), rows * 8),
+           ("HyperLogLog distinct estimate (int32 keys)", lambda: gx.compute_ndv_approx(k), rows * 4),
+           ("filter: int64 BETWEEN keeping 1/2, compaction of both columns", lambda: gx.select([k, v], half),
+            pair + pair // 2)]
+    out = []
+    for desc, fn, alg in ops:
+        ms = time_steps(torch, fn, 3, 2, dist) / 3
+        out.append({"op": desc, "ms": round(ms, 3), "grows_s": round(rows / ms / 1e6, 2),
+                    "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)})
+    del k, v
+    torch.cuda.empty_cache()
     return out
 
 
