@@ -304,6 +304,36 @@ __host__ __device__ __forceinline__ uint64_t ordered64(uint64_t b, int kind) {
     return b;
 }
 
+// Radix-sort digit source: the order-preserving image of a key (narrow keys
+// widened to 4 bytes carry their logical width), inverted for a descending
+// sort, minus a bias (a sort on the bits the keys span).
+struct img_params {
+    int kind;      // vkind of the key type
+    int lw;        // logical key width in bytes (1, 2, 4, 8)
+    int desc;      // descending
+    uint64_t bias; // subtracted from the image before digit extraction
+};
+
+template <int KW>
+__host__ __device__ __forceinline__ uint64_t key_image(uint64_t raw, const img_params& ip) {
+    uint64_t img;
+    if (KW == 4) {
+        uint32_t b = (uint32_t)raw;
+        if (ip.lw < 4) {
+            b &= (1u << (8 * ip.lw)) - 1u;
+            if (ip.kind == VK_I) b ^= 1u << (8 * ip.lw - 1);
+        } else {
+            b = ordered32(b, ip.kind);
+        }
+        img = b;
+        if (ip.desc) img = (~img) & 0xFFFFFFFFull;
+    } else {
+        img = ordered64(raw, ip.kind);
+        if (ip.desc) img = ~img;
+    }
+    return img - ip.bias;
+}
+
 // ---------------------------------------------------------------------------
 // Small helpers.
 // ---------------------------------------------------------------------------

@@ -70,6 +70,11 @@ inline int key_bits(int type) { return 8 * size_of(type); }
 
 // Min/max of the order-preserving image (for trimming radix passes).
 void key_image_range(const col& keys, uint64_t* lo, uint64_t* hi, cudaStream_t s);
+// One stable radix-sort digit pass through the partition plan's bulk-copy
+// scatter (gx_groupby_partition.cu); false when it does not apply.
+bool radix_pass_bulk(const void* kin, const void* vin, int kw, int vw, bool iota, int64_t n, const img_params& ip,
+                     int shift, int dbits, int tile_rows, const int64_t* offs, void* kout, void* vout, int* err,
+                     cudaStream_t s);
 
 // ----- statistics (gx_hll.cu) -----
 int64_t ndv_estimate(const col& key, cudaStream_t s);

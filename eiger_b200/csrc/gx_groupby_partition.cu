@@ -307,9 +307,12 @@ __host__ __device__ inline pb_layout pb_make_layout(const move_cols& mc, bool st
     return L;
 }
 
-template <int KW, int NC, bool STABLE>
+// IMG: the digit is bits [shift, shift + dbits) of the key's order-preserving
+// image (a stable LSD radix-sort pass, `ip`); otherwise of the key's
+// partition hash (`kind`).
+template <int KW, int NC, bool STABLE, bool IMG>
 __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __restrict__ keys, int64_t n, int kind,
-                                                                int shift, int dbits, int64_t ntiles,
+                                                                img_params ip, int shift, int dbits, int64_t ntiles,
                                                                 const int64_t* __restrict__ offsets, move_cols mc,
                                                                 pb_layout L, int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char pb_smem[];
@@ -345,8 +348,10 @@ __global__ void __launch_bounds__(PB_NT, 1) k_part_scatter_bulk(const void* __re
     // Digit of the tile's row `local` (key column of the current stage).
     auto digit_at = [&](int local) -> unsigned {
         uint64_t kb;
-        if (KW == 4) kb = canon32(reinterpret_cast<const unsigned*>(stage + L.in_off[0])[local], kind);
-        else kb = canon64(reinterpret_cast<const unsigned long long*>(stage + L.in_off[0])[local], kind);
+        if (KW == 4) kb = reinterpret_cast<const unsigned*>(stage + L.in_off[0])[local];
+        else kb = reinterpret_cast<const unsigned long long*>(stage + L.in_off[0])[local];
+        if constexpr (IMG) return (unsigned)((key_image<KW>(kb, ip) >> shift) & (uint64_t)(bins - 1));
+        kb = KW == 4 ? canon32((uint32_t)kb, kind) : canon64(kb, kind);
         return (part_hash<KW>(kb) >> shift) & (bins - 1);
     };
     if (t == 0) {
@@ -795,11 +800,11 @@ void partition_starts(const void* keys, int kw, int64_t n, int kind, int R, int6
 
 namespace {
 
-// The bulk-copy scatter applies to 2..4 moved columns when every loaded
+// The bulk-copy scatter applies to 1..4 moved columns when every loaded
 // column is 4 or 8 bytes wide and 16-byte aligned, and two tiles of them fit
 // in shared memory (four columns: up to 24 B per row, single-pass ranking).
 static bool bulk_scatter_ok(const move_cols& mc, const pb_layout& L) {
-    if (getenv("GX_PART_NO_BULK") || mc.n < 2 || mc.n > 4) return false;
+    if (mc.n < 1 || mc.n > 4) return false;
     for (int c = 0; c < mc.n; ++c) {
         if (mc.iota[c]) continue;
         if (mc.width[c] != 4 && mc.width[c] != 8) return false;
@@ -817,21 +822,23 @@ void part_pass(const void* kin, int64_t n, int kind, int shift, int dbits, move_
     GX_LAUNCHED();
     exclusive_scan_i64(counts, offs, ((int64_t)1 << dbits) * ntiles, s);
     const pb_layout L = pb_make_layout(mc, stable);
-    if (bulk_scatter_ok(mc, L)) {
+    if (mc.n >= 2 && !getenv("GX_PART_NO_BULK") && bulk_scatter_ok(mc, L)) {
         static per_device_flag battr;
         battr.once([] {
             const int lim = dev().max_smem_optin - 2048;
-            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 3, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 4, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<KW, 4, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
         });
         const int grid = (int)std::min<int64_t>(ntiles, dev().sm_count);
+        const img_params no_img{};
         GX_PROF("partition_scatter", s);
-#define GX_PB_LAUNCH(NCV, ST) \
-    k_part_scatter_bulk<KW, NCV, ST><<<grid, PB_NT, L.total, s>>>(kin, n, kind, shift, dbits, ntiles, offs, mc, L, err)
+#define GX_PB_LAUNCH(NCV, ST)                                                                                       \
+    k_part_scatter_bulk<KW, NCV, ST, false><<<grid, PB_NT, L.total, s>>>(kin, n, kind, no_img, shift, dbits, ntiles, \
+                                                                          offs, mc, L, err)
         if (mc.n == 2 && stable) GX_PB_LAUNCH(2, true);
         else if (mc.n == 2) GX_PB_LAUNCH(2, false);
         else if (mc.n == 3 && stable) GX_PB_LAUNCH(3, true);
@@ -1075,6 +1082,45 @@ void partition_groupby(const col& key_in, const agg_plan& p, gx_groupby_hint* hi
 // every key with its row id.  keys_out / rows_out hold n entries; partition
 // p is rows [part_start[p], part_start[p + 1]) of them (2^R + 1 starts).
 // Row order inside a partition is unspecified.
+// One stable LSD radix-sort pass through the bulk-copy scatter (digit =
+// bits [shift, shift + dbits) of the key image), for 4/8-byte keys and
+// optional 4/8-byte values or row ids, every loaded column starting on a
+// 16-byte boundary: `offs` are the scanned digit counts [digit][tile] of
+// `tile_rows`-row tiles.  Returns false, launching nothing, when the pass
+// does not fit the kernel; sets *err when a bulk copy never completed.
+bool radix_pass_bulk(const void* kin, const void* vin, int kw, int vw, bool iota, int64_t n, const img_params& ip,
+                     int shift, int dbits, int tile_rows, const int64_t* offs, void* kout, void* vout, int* err,
+                     cudaStream_t s) {
+    if (getenv("GX_RADIX_NO_BULK") || tile_rows != PS_TILE || n <= 0) return false;
+    if ((kw != 4 && kw != 8) || (vw != 0 && vw != 4 && vw != 8) || (iota && vw != 8)) return false;
+    move_cols mc;
+    std::memset(&mc, 0, sizeof(mc));
+    mc.n = vw ? 2 : 1;
+    mc.in[0] = kin; mc.width[0] = kw; mc.out[0] = kout;
+    if (vw) { mc.in[1] = iota ? nullptr : vin; mc.width[1] = vw; mc.iota[1] = iota ? 1 : 0; mc.out[1] = vout; }
+    const pb_layout L = pb_make_layout(mc, true);
+    if (!bulk_scatter_ok(mc, L)) return false;
+    static per_device_flag battr;
+    battr.once([] {
+        const int lim = dev().max_smem_optin - 2048;
+        GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<4, 1, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<4, 2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<8, 1, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        GX_CUDA(cudaFuncSetAttribute(k_part_scatter_bulk<8, 2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    });
+    const int64_t ntiles = ceil_div(n, PS_TILE);
+    const int grid = (int)std::min<int64_t>(ntiles, dev().sm_count);
+#define GX_RB_LAUNCH(K, NCV) \
+    k_part_scatter_bulk<K, NCV, true, true><<<grid, PB_NT, L.total, s>>>(kin, n, ip.kind, ip, shift, dbits, ntiles, offs, mc, L, err)
+    if (kw == 4 && mc.n == 1) GX_RB_LAUNCH(4, 1);
+    else if (kw == 4) GX_RB_LAUNCH(4, 2);
+    else if (mc.n == 1) GX_RB_LAUNCH(8, 1);
+    else GX_RB_LAUNCH(8, 2);
+#undef GX_RB_LAUNCH
+    GX_LAUNCHED();
+    return true;
+}
+
 void hash_partition_rows(const col& key, int R, void* keys_out, int64_t* rows_out, int64_t* part_start,
                          cudaStream_t s) {
     const int64_t n = key.n;

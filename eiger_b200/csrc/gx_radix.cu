@@ -30,33 +30,6 @@ constexpr int RS_TILE = RS_NT * RS_IPT;
 constexpr int RS_MAXBITS = 8;
 constexpr int RS_BINS = 1 << RS_MAXBITS;
 
-struct img_params {
-    int kind;      // vkind of the key type
-    int lw;        // logical key width in bytes (1, 2, 4, 8)
-    int desc;      // descending
-    uint64_t bias; // subtracted from the image before digit extraction
-};
-
-template <int KW>
-__device__ __forceinline__ uint64_t key_image(uint64_t raw, const img_params& ip) {
-    uint64_t img;
-    if (KW == 4) {
-        uint32_t b = (uint32_t)raw;
-        if (ip.lw < 4) {
-            b &= (1u << (8 * ip.lw)) - 1u;
-            if (ip.kind == VK_I) b ^= 1u << (8 * ip.lw - 1);
-        } else {
-            b = ordered32(b, ip.kind);
-        }
-        img = b;
-        if (ip.desc) img = (~img) & 0xFFFFFFFFull;
-    } else {
-        img = ordered64(raw, ip.kind);
-        if (ip.desc) img = ~img;
-    }
-    return img - ip.bias;
-}
-
 template <int KW>
 __device__ __forceinline__ uint64_t load_key(const void* p, int64_t i) {
     if (KW == 4) return __ldg(static_cast<const unsigned*>(p) + i);
@@ -269,11 +242,12 @@ __global__ void k_narrow(D* __restrict__ out, const S* __restrict__ in, int64_t 
 size_t radix_temp_bytes(int64_t n, int key_width, int val_width) {
     int kw = key_width < 4 ? 4 : key_width;
     int64_t ntiles = ceil_div(std::max<int64_t>(n, 1), RS_TILE);
-    // Six sub-buffers, each rounded up to 256 bytes: 6 * 256 of slack.
+    // Seven sub-buffers (the last an error flag), each rounded up to 256
+    // bytes: 7 * 256 of slack.
     size_t b = (size_t)n * (kw + val_width);
     b += (size_t)RS_BINS * ntiles * 8 * 2 + 8;
     if (key_width < 4) b += (size_t)n * 4 * 2;
-    return b + 6 * 256 + 256;
+    return b + 7 * 256 + 256;
 }
 
 void key_image_range(const col& keys, uint64_t* lo, uint64_t* hi, cudaStream_t s) {
@@ -355,6 +329,9 @@ void radix_sort_biased(const col& keys_c, const void* vals_in, int val_width, bo
         char* tv = val_width ? take((size_t)n * val_width) : nullptr;
         int64_t* counts = reinterpret_cast<int64_t*>(take((size_t)RS_BINS * ntiles * 8));
         int64_t* offs = reinterpret_cast<int64_t*>(take((size_t)RS_BINS * ntiles * 8 + 8));
+        int* err = reinterpret_cast<int*>(take(8));
+        GX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+        bool bulk = false;
         const void* kin = keys.data;
         const void* vin = vals_in;
         bool iota = vals_iota;
@@ -370,12 +347,18 @@ void radix_sort_biased(const col& keys_c, const void* vals_in, int val_width, bo
             int64_t bins = 1 << dbits;
             exclusive_scan_i64(counts, offs, bins * ntiles, s);
             GX_PROF("radix_scatter", s);
-            scatter_dispatch(kw, val_width, iota, ntiles, s, kin, vin, n, ip, shift, dbits, offs, ko, vo);
+            // Persistent bulk-copy pass where the columns allow it (16-byte
+            // aligned 4/8-byte keys and values), else the per-tile kernel.
+            if (radix_pass_bulk(kin, vin, kw, val_width, iota, n, ip, shift, dbits, RS_TILE, offs, ko, vo, err, s))
+                bulk = true;
+            else
+                scatter_dispatch(kw, val_width, iota, ntiles, s, kin, vin, n, ip, shift, dbits, offs, ko, vo);
             kin = ko;
             vin = vo;
             iota = false;
             shift += dbits;
         }
+        if (bulk && read_scalar(err, s)) fail(GX_ETIMEOUT, "radix sort: a bulk copy into shared memory did not complete");
     }
     if (lw < 4) {
         int g = grid_for(n, 256, 8);

@@ -34,6 +34,32 @@ def test_sort_pairs_bit_exact(kdt, bits, desc):
     assert np.array_equal(sv.cpu().numpy(), ev)
 
 
+@pytest.mark.parametrize("per_tile", [False, True])
+@pytest.mark.parametrize("kdt,vdt", [(np.int32, np.int64), (np.float64, np.int32), (np.uint64, np.float64)])
+def test_sort_pairs_persistent_and_per_tile_passes(monkeypatch, per_tile, kdt, vdt):
+    # Several tiles per SM and a partial last tile, through the persistent
+    # bulk-copy digit passes and through the per-tile kernel
+    # (GX_RADIX_NO_BULK): both bit-exact, ascending and descending, on a bit
+    # range and on row ids.
+    if per_tile:
+        monkeypatch.setenv("GX_RADIX_NO_BULK", "1")
+    n = 148 * 3 * 4096 + 1234
+    if np.dtype(kdt).kind == "f":
+        k = (O.gen_values(n, np.float64, seed=5) * 2000 - 1000).astype(kdt)
+    else:
+        k = O.gen_keys(n, np.int64, groups=1 << 40, seed=6).astype(kdt)
+    v = O.gen_values(n, np.int64, lo=0, hi=1 << 30, seed=7).astype(vdt)
+    for b, e, desc in ((0, -1, False), (0, -1, True), (3, 21, False)):
+        sk, sv = gx.sort_column_pair(to_dev(k), to_dev(v), b, e, gx.DESCENDING if desc else gx.ASCENDING)
+        ek, ev = O.sort_pairs(k, v, b, e, desc)
+        assert np.array_equal(sk.cpu().numpy().view(np.uint8), ek.view(np.uint8))
+        assert np.array_equal(sv.cpu().numpy().view(np.uint8), ev.view(np.uint8))
+    sk, idx = gx.argsort(to_dev(k))
+    ek, ei = O.sort_pairs(k, iota=True)
+    assert np.array_equal(sk.cpu().numpy().view(np.uint8), ek.view(np.uint8))
+    assert np.array_equal(idx.cpu().numpy(), ei)
+
+
 @pytest.mark.parametrize("n", [0, 1, 4095, 4096, 4097, 1 << 20])
 def test_argsort_and_sort_column(n):
     k = O.gen_keys(n, np.int64, groups=1000, scatter=1, seed=4) if n else np.zeros(0, np.int64)
