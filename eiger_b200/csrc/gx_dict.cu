@@ -76,15 +76,41 @@ __device__ __forceinline__ int64_t d_find(const dtable& t, uint64_t k, bool inse
     return -1;
 }
 
+// Rows per thread per round of the insert and lookup kernels: their keys are
+// loaded, then their home slots probed, all at once, so each thread keeps
+// DU independent table reads in flight instead of one dependent chain.
+constexpr int DU = 4;
+
+// Slot of key k when it sits in its home slot (one plain load), else -1.
+// A stale read (the key being inserted by another thread) only sends the
+// row to the full probe walk.
+template <int KW>
+__device__ __forceinline__ int64_t d_home(const dtable& t, uint64_t k) {
+    if (KW == 8 && k == D_EMPTY8) return -1;
+    const uint64_t slot = dhash<KW>(k) & t.mask;
+    return t.keys[slot] == k ? (int64_t)slot : -1;
+}
+
 template <int KW>
 __global__ void k_dict_insert(const void* __restrict__ keys, int64_t n, int kind, dtable t, int assign,
                               unsigned long long* __restrict__ counter) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        bool ins;
-        int64_t s = d_find<KW>(t, dkey<KW>(keys, i, kind), true, &ins);
-        if (ins) {
-            unsigned long long c = atomicAdd(counter, 1ull);
-            if (assign) t.codes[s] = c;
+    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < n; i0 += step * DU) {
+        uint64_t k[DU];
+        int64_t home[DU];
+#pragma unroll
+        for (int q = 0; q < DU; ++q) k[q] = i0 + q * step < n ? dkey<KW>(keys, i0 + q * step, kind) : 0;
+#pragma unroll
+        for (int q = 0; q < DU; ++q) home[q] = i0 + q * step < n ? d_home<KW>(t, k[q]) : 0;
+#pragma unroll
+        for (int q = 0; q < DU; ++q) {
+            if (i0 + q * step >= n || home[q] >= 0) continue;
+            bool ins;
+            int64_t s = d_find<KW>(t, k[q], true, &ins);
+            if (ins) {
+                unsigned long long c = atomicAdd(counter, 1ull);
+                if (assign) t.codes[s] = c;
+            }
         }
     }
 }
@@ -111,11 +137,26 @@ __device__ __forceinline__ void store_code(void* out, int w, int64_t i, uint64_t
 template <int KW>
 __global__ void k_dict_lookup(const void* __restrict__ keys, int64_t n, int kind, dtable t, void* out, int ow,
                               uint64_t missing) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        bool ins;
-        int64_t s = d_find<KW>(t, dkey<KW>(keys, i, kind), false, &ins);
-        uint64_t c = s >= 0 ? t.codes[s] : NO_CODE;
-        store_code(out, ow, i, c == NO_CODE ? missing : c);
+    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < n; i0 += step * DU) {
+        uint64_t k[DU];
+        int64_t slot[DU];
+#pragma unroll
+        for (int q = 0; q < DU; ++q) k[q] = i0 + q * step < n ? dkey<KW>(keys, i0 + q * step, kind) : 0;
+#pragma unroll
+        for (int q = 0; q < DU; ++q) slot[q] = i0 + q * step < n ? d_home<KW>(t, k[q]) : 0;
+#pragma unroll
+        for (int q = 0; q < DU; ++q) {
+            if (i0 + q * step >= n || slot[q] >= 0) continue;
+            bool ins;
+            slot[q] = d_find<KW>(t, k[q], false, &ins);
+        }
+        uint64_t c[DU];
+#pragma unroll
+        for (int q = 0; q < DU; ++q) c[q] = i0 + q * step < n && slot[q] >= 0 ? t.codes[slot[q]] : NO_CODE;
+#pragma unroll
+        for (int q = 0; q < DU; ++q)
+            if (i0 + q * step < n) store_code(out, ow, i0 + q * step, c[q] == NO_CODE ? missing : c[q]);
     }
 }
 

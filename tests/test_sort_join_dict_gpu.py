@@ -265,6 +265,25 @@ def test_dictionary_encode(kdt, et, ndv):
         assert np.array_equal(oc.cpu().numpy().astype(np.int64), ec.astype(np.dtype(gx._NP[et])).astype(np.int64))
 
 
+def test_dictionary_encode_marker_key_and_ragged_rows():
+    # INT64_MIN (the 8-byte table's empty marker, kept in a side slot) among
+    # the keys, and a row count that leaves a partial round of rows per thread.
+    n = (1 << 20) + 13
+    k = O.gen_keys(n, np.int64, groups=3000, scatter=1, seed=77)
+    k[::1001] = np.iinfo(np.int64).min
+    codes, nd = gx.dictionary_encode(to_dev(k), gx.INT32)
+    c = codes.cpu().numpy().astype(np.int64)
+    assert nd == len(np.unique(k))
+    assert set(c.tolist()) == set(range(nd))
+    assert len(set(zip(k.tolist(), c.tolist()))) == nd
+    oc, _ = gx.dictionary_encode(to_dev(k), gx.INT32, ordered=True)
+    ec, _ = O.dict_encode(k, ordered=True)
+    assert np.array_equal(oc.cpu().numpy().astype(np.int64), ec.astype(np.int64))
+    d = np.unique(k)[::-1].copy()
+    got = gx.dictionary_encode_with_dict(to_dev(k), to_dev(d)).cpu().numpy()
+    assert np.array_equal(got, O.dict_with_dict(k, d))
+
+
 def test_dictionary_encode_with_dict():
     d = O.gen_perm(4096, np.int32, seed=5, base=-2048)
     q = O.gen_keys(1 << 18, np.int32, groups=5000, seed=6) - 2048
