@@ -390,15 +390,24 @@ def run_gx(args) -> None:
         l0 = gx.kernel_launches()
         p_ms = time_steps(torch, plan.run_per_instance, nsteps, 3, dist) / nsteps
         p_launches = (gx.kernel_launches() - l0) // (nsteps + 3)
-        # Algorithmic bytes: every instance's strings, offsets, dates and amounts once.
+        # Input bytes: every instance's strings, offsets, dates and amounts
+        # once (what the per-instance engine reads).  Must-read bytes of a
+        # plan that applies the date range first: dates and offsets of every
+        # row, strings and amounts of the kept rows only.
         in_b = sum(int(it.offsets[-1].item()) + (it.rows + 1) * 8 + it.rows * 12 for it in insts)
+        need_b = 0
+        for it in insts:
+            keep = (it.date >= it.lo) & (it.date < it.hi)
+            lens = it.offsets[1:] - it.offsets[:-1]
+            need_b += (it.rows + 1) * 8 + it.rows * 4 + int((lens * keep).sum().item()) + 8 * int(keep.sum().item())
         batched = {
             "workload": (f"{len(insts)} string group-by pipelines, rows log-uniform in [2^12, 2^22] "
                          f"({total} rows total): dictionary-encode ASCII keys (10^4 distinct, 8..32 bytes), "
                          "keep 40% of rows by a date range, SUM(int64 scale-2 decimal) + COUNT per key"),
-            "rows": total, "input_bytes": in_b,
+            "rows": total, "input_bytes": in_b, "must_read_bytes": need_b,
             "batched": {"ms_per_step": b_ms, "value": world * total / (b_ms * 1e-3) / 1e6, "unit": "Mrows/s",
-                        "launches_per_step": b_launches, "hbm_frac": in_b / (b_ms * 1e-3) / 1e9 / peaks["hbm_gbs"]},
+                        "launches_per_step": b_launches, "hbm_frac": in_b / (b_ms * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                        "hbm_frac_must_read": need_b / (b_ms * 1e-3) / 1e9 / peaks["hbm_gbs"]},
             "per_instance": {"ms_per_step": p_ms, "value": world * total / (p_ms * 1e-3) / 1e6, "unit": "Mrows/s",
                              "launches_per_step": p_launches},
             "speedup": p_ms / b_ms, "tile_rows": tile, "load_factor_pct": lf,

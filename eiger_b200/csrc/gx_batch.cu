@@ -15,7 +15,9 @@
 // single CAS publishes a new entry and the bytes are compared against the
 // representative row of the input, both read as 8-byte chunks of aligned
 // words — gets the next dictionary code on insert, and adds its amount /
-// count to the slot when it passes the date filter.  A finalize kernel
+// count to the slot.  The date filter runs first: only kept rows are
+// encoded (the output holds kept groups only), so the dictionary and its
+// codes cover the kept rows' strings.  A finalize kernel
 // writes the per-code results.  Both kernels and the resets are captured
 // once into a CUDA graph and replayed.  Tile size and table load factor are
 // chosen by timing the candidates on the batch.
@@ -295,11 +297,16 @@ __global__ void __launch_bounds__(256, 4) k_batch_main(batch_dev b) {
                 ndt = in.date[rn];
                 nam = in.amount[rn];
             }
-            bool ins;
-            const int64_t slot = find_or_insert<true>(b, in, it.inst, r, o0, o1 - o0, &ins);
-            if (slot >= 0 && dt >= in.lo && dt < in.hi) {
-                atomicAdd(&b.sum_slot[slot], (unsigned long long)am);
-                atomicAdd(&b.cnt_slot[slot], 1ull);
+            // The date range is applied before the string is encoded: the
+            // output covers kept rows only, so a dropped row needs no hash,
+            // probe or string bytes (its codes would never be read).
+            if (dt >= in.lo && dt < in.hi) {
+                bool ins;
+                const int64_t slot = find_or_insert<true>(b, in, it.inst, r, o0, o1 - o0, &ins);
+                if (slot >= 0) {
+                    atomicAdd(&b.sum_slot[slot], (unsigned long long)am);
+                    atomicAdd(&b.cnt_slot[slot], 1ull);
+                }
             }
             o0 = n0;
             o1 = n1;

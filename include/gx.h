@@ -580,7 +580,8 @@ typedef struct gx_batch_plan gx_batch_plan;
 
 /* Plan a batch: validates the descriptors, runs the autotuner (tile rows,
  * table load factor) and sizes per-instance tables.  `max_distinct` bounds
- * the dictionary of every instance. */
+ * the dictionary of every instance (gx_batch_run encodes the strings of the
+ * rows its date range keeps; the per-instance engine encodes every row). */
 gx_status gx_batch_plan_create(const gx_batch_instance* instances, int32_t count,
                                int64_t max_distinct, gx_stream_t stream,
                                gx_batch_plan** plan);

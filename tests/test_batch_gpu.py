@@ -42,6 +42,22 @@ def test_repeated_runs_of_one_plan():
         assert plan.results() == exp
 
 
+@pytest.mark.parametrize("keep", [0.0, 1.0])
+def test_date_range_keeping_none_or_all(keep):
+    # The batched launch applies the date range before encoding: a range
+    # that keeps no row leaves every instance without groups, one that keeps
+    # every row groups all of them; the per-instance engine (encode first)
+    # agrees in both cases.
+    insts, _ = B.make_instances(12, seed=23, min_log2=8, max_log2=14, dict_size=1500, keep=keep)
+    exp = expected(insts)
+    assert all(len(e) == 0 for e in exp) if keep == 0.0 else all(len(e) > 0 for e in exp)
+    plan = B.Plan(insts, max_distinct=1500)
+    plan.run()
+    assert plan.results() == exp
+    plan.run_per_instance()
+    assert plan.results() == exp
+
+
 def test_empty_and_tiny_instances():
     insts, _ = B.make_instances(5, seed=9, min_log2=0, max_log2=3, dict_size=50)
     plan = B.Plan(insts, max_distinct=50)
