@@ -536,19 +536,37 @@ def operators_grid(gx, torch, rows: int, peaks: dict, dist=None) -> list:
     [0, 2^31)): radix sort and 8-bit radix partition of (key, value) pairs,
     dictionary encode, the HyperLogLog distinct estimate, and a BETWEEN
     filter keeping half the rows with the compaction of both columns.  Per
-    operator: ms, Grows/s and the fraction of measured HBM for its
-    algorithmic bytes (inputs read once, outputs written once; a 4-pass sort
-    moves about four times that)."""
+    operator (its C-ABI call): ms, Grows/s and the fraction of measured HBM
+    for its algorithmic bytes (inputs read once, outputs written once; a
+    4-pass sort moves about four times that)."""
     k = torch.empty(rows, dtype=torch.int32, device="cuda")
     gx.generate_keys(k, gx.gen_spec(seed=11, groups=1 << 16, scatter=1))
     v = torch.empty(rows, dtype=torch.int64, device="cuda")
     gx.generate_values(v, gx.gen_spec(seed=11, stream_id=1, lo=0, hi=1 << 31))
     pair = rows * (4 + 8)
     half = [gx.predicate(1, gx.CMP_BETWEEN, 0, 1 << 30)]
-    ops = [("radix sort, 32 key bits (int32 key, int64 value)", lambda: gx.sort_column_pair(k, v), 2 * pair),
-           ("radix partition, 8 bits (int32 key, int64 value)", lambda: gx.partition_column_pair(k, v, 0, 8),
-            2 * pair),
-           ("dictionary encode (int32 keys -> int32 codes)", lambda: gx.dictionary_encode(k), rows * 8),
+    import ctypes
+    kv, vv = gx.view(k), gx.view(v)
+
+    # Each operator through its C-ABI call, as a C caller sees it: outputs
+    # stay in the library's buffers and are freed after the call (the Python
+    # wrappers' copies into torch tensors are not the operator).
+    def c_pair(fn, *args):
+        ko, vo = gx.OwnedColumn(), gx.OwnedColumn()
+        gx.check(fn(kv, vv, *args, None, 0, None, ctypes.byref(ko), ctypes.byref(vo)))
+        gx.check(gx.lib.gx_free(ko.data, None))
+        gx.check(gx.lib.gx_free(vo.data, None))
+
+    def c_dict():
+        o, nd = gx.OwnedColumn(), ctypes.c_int64()
+        gx.check(gx.lib.gx_dictionary_encode(kv, gx.INT32, 0, 0.25, None, ctypes.byref(o), ctypes.byref(nd)))
+        gx.check(gx.lib.gx_free(o.data, None))
+
+    ops = [("radix sort, 32 key bits (int32 key, int64 value)",
+            lambda: c_pair(gx.lib.gx_sort_column_pair, 0, -1, gx.ASCENDING), 2 * pair),
+           ("radix partition, 8 bits (int32 key, int64 value)",
+            lambda: c_pair(gx.lib.gx_partition_column_pair, 0, 8), 2 * pair),
+           ("dictionary encode (int32 keys -> int32 codes)", c_dict, rows * 8),
            ("HyperLogLog distinct estimate (int32 keys)", lambda: gx.compute_ndv_approx(k), rows * 4),
            ("filter: int64 BETWEEN keeping 1/2, compaction of both columns", lambda: gx.select([k, v], half),
             pair + pair // 2)]
