@@ -483,8 +483,8 @@ def shapes_grid(gx, torch, rows: int, peaks: dict, sel: int, dist=None) -> list:
     """Group-by requests outside the compiled aggregation plans, through
     AUTO at `rows` rows: a run-time aggregation list over the int64 + float64
     columns (2^16 and 2^10 groups), and three value columns (int64, float64,
-    int32), whose rows of four moved columns take the register-staged
-    partition scatter.  Per shape: AUTO's pick with its ms, Grows/s and
+    int32: four moved columns, 24 B per row, in the partition scatter).  Per
+    shape: AUTO's pick with its ms, Grows/s and
     fraction of measured HBM (algorithmic bytes: every input column read
     once plus the output records), and the ms of HASH and PARTITION forced."""
     names = {gx.HASH: "hash", gx.SORT: "sort", gx.SORT_OPT: "sort_opt", gx.SORT_GFUR: "sort_gfur",

@@ -358,8 +358,9 @@ def test_forced_alternative_kernels(monkeypatch, env, algo, G):
 def test_many_value_columns(algo, G, ncols):
     # Run-time aggregation lists over three or five value columns of mixed
     # widths: the dense-id unit kernel takes up to four columns, the
-    # slot-indexed one (or HASH's shared-table kernel) more, and PARTITION
-    # moves more than three columns through the register-staged scatter.
+    # slot-indexed one (or HASH's shared-table kernel) more; PARTITION moves
+    # four columns (24 B per row) through the bulk-copy scatter and six
+    # through the register-staged one.
     n = (1 << 19) + 77
     key = O.gen_keys(n, np.int32, groups=G, scatter=1, seed=61)
     cols = [O.gen_values(n, np.int64, lo=-(1 << 40), hi=1 << 40, seed=62),
