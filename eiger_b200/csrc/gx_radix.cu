@@ -12,10 +12,14 @@
 //   1. k_radix_hist  — one CTA per 4096-row tile, shared-memory histogram,
 //                      counts written bin-major [bin][tile];
 //   2. exclusive scan of the counts -> global start of (bin, tile);
-//   3. k_radix_scatter — warp-level multisplit (match.any ranks rows with
-//                      equal digits in input order), tile reordered by digit
-//                      in shared memory, then written out in digit runs so
-//                      each run is a contiguous, coalesced store.
+//   3. scatter — where keys and values are 16-byte aligned 4/8-byte
+//                      columns, the persistent bulk-copy scatter of the
+//                      partition plan (radix_pass_bulk, key-image digits,
+//                      stable ranking); otherwise k_radix_scatter: warp-level
+//                      multisplit (match.any ranks rows with equal digits in
+//                      input order), tile reordered by digit in shared
+//                      memory, then written out in digit runs so each run is
+//                      a contiguous, coalesced store.
 #include <algorithm>
 
 #include "gx_groupby.h"
